@@ -1,0 +1,375 @@
+"""polyhomocont_b200 -- B200 path tracker for polyhomocont's solve().
+
+Python mirror of the reference's Fortran API over the C ABI of
+libphc_b200.so (include/polyhomocont_b200.h):
+
+    type(sparse_system)   -> SparseSystem   (init, add_equation, nvars, ...)
+    type(solve_options)   -> SolveOptions   (tracker, endgame, seed, tolerances)
+    solve(sys, res, status, options) -> res, status = solve(sys, options)
+    type(solve_result)    -> SolveResult    (paths, solutions, counts, ...)
+
+The per-path numerics run on the GPU (one warp per path, sm_100a); the
+order-dependent bookkeeping runs on the host in path order, as in the
+reference. There is no CPU fallback: without the built library or a CUDA
+device the calls raise.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import (PATH_DTYPE, PHC_ERR_INVALID_INPUT, PHC_OK, PHC_PREC_FP64,  # noqa: F401
+                   PHC_PREC_MIXED, PHC_SCHED_GRID, PHC_SCHED_PERSISTENT, EndgameOptions,
+                   GpuOptions, SolveOptions, TrackerOptions)
+
+STATUS_OK = 0
+ERR_INVALID_INPUT = 1
+ERR_SINGULAR_MATRIX = 2
+ERR_NUMERICAL = 3
+PATH_SUCCESS = 0
+PATH_FAILED_MIN_STEP = 1
+PATH_FAILED_MAX_STEPS = 2
+PATH_ENDGAME_FAILED = 3
+ENDGAME_CONVERGED = 0
+ENDGAME_NOT_CONVERGED = 1
+
+
+class PhcError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__(f"{what} failed with status {code}: {_abi.last_error()}")
+        self.code = code
+
+
+def _check_device_status(st, what):
+    """Negative codes are device/runtime errors: raise. Codes 0..3 are the
+    reference's solve statuses and are returned to the caller."""
+    if st < 0:
+        raise PhcError(st, what)
+    return st
+
+
+def default_options():
+    o = SolveOptions()
+    _abi.lib().phc_default_solve_options(ctypes.byref(o))
+    return o
+
+
+def default_gpu_options(precision=PHC_PREC_MIXED, schedule=PHC_SCHED_PERSISTENT, device=0,
+                        warps_per_block=0):
+    g = GpuOptions()
+    _abi.lib().phc_default_gpu_options(ctypes.byref(g))
+    g.precision = precision
+    g.schedule = schedule
+    g.device = device
+    g.warps_per_block = warps_per_block
+    return g
+
+
+class SparseSystem:
+    """type(sparse_system), src/sparse.f90:31-61"""
+
+    def __init__(self, n=None):
+        self._L = _abi.lib()
+        self.h = self._L.phc_sparse_create()
+        if not self.h:
+            raise MemoryError("phc_sparse_create")
+        if n is not None:
+            self.init(n)
+
+    def __del__(self):
+        try:
+            self._L.phc_sparse_destroy(self.h)
+        except Exception:
+            pass
+
+    def init(self, n):
+        """sys%init(n), src/sparse.f90:65-81"""
+        return self._L.phc_sparse_init(self.h, int(n))
+
+    def add_equation(self, coefs, exps):
+        """sys%add_equation(coefs, exps, status), src/sparse.f90:83-141.
+        exps: (rows, cols) exponent matrix, one column per term."""
+        c = np.ascontiguousarray(np.asarray(coefs, dtype=np.complex128).ravel())
+        e = np.asarray(exps, dtype=np.int32)
+        if e.ndim == 1:
+            e = e.reshape(-1, 1)
+        flat = np.ascontiguousarray(e.ravel(order="F"))
+        cd = c.view(np.float64)
+        return self._L.phc_sparse_add_equation(self.h, c.size, _abi.dptr(cd), e.shape[0],
+                                               e.shape[1], _abi.iptr(flat))
+
+    def nvars(self):
+        return self._L.phc_sparse_nvars(self.h)
+
+    def nequations(self):
+        return self._L.phc_sparse_nequations(self.h)
+
+    def nterms(self, i):
+        return self._L.phc_sparse_nterms(self.h, int(i))
+
+    def total_terms(self):
+        return self._L.phc_sparse_total_terms(self.h)
+
+    def degrees(self):
+        d = np.zeros(max(self.nequations(), 1), dtype=np.int32)
+        self._L.phc_sparse_degrees(self.h, _abi.iptr(d))
+        return d[:self.nequations()]
+
+    def table(self):
+        """phc_system view of the packed table and its status (err_invalid_input
+        if the system does not have n equations)."""
+        t = _abi.SystemC()
+        st = self._L.phc_sparse_table(self.h, ctypes.byref(t))
+        return t, st
+
+    def bezout(self):
+        t, st = self.table()
+        return int(self._L.phc_bezout(ctypes.byref(t))) if st == 0 else 0
+
+
+class SolveResult:
+    """type(solve_result), src/solve.f90:121-150. Arrays are 0-based with
+    solutions as rows; the path index fields keep the reference's 1-based
+    meaning (0 = none)."""
+
+    def __init__(self):
+        self.n = 0
+        self.npaths = 0
+        self.paths = np.zeros(0, dtype=PATH_DTYPE)
+        self.z = np.zeros((0, 1), dtype=np.complex128)
+        self.x = np.zeros((0, 1), dtype=np.complex128)
+        self.nsolutions = 0
+        self.solutions = np.zeros((0, 0), dtype=np.complex128)
+        self.nreal = 0
+        self.real_solutions = np.zeros((0, 0))
+        self.nsingular = 0
+        self.singular_solutions = np.zeros((0, 0), dtype=np.complex128)
+        self.multiplicities = np.zeros(0, dtype=np.int32)
+        self.ninfinite = 0
+        self.nfailed = 0
+        self.nduplicates = 0
+
+
+def _result_buffers(n, npaths):
+    m = max(npaths, 1)
+    nn = max(n, 1)
+    bufs = dict(
+        paths=np.zeros(m, dtype=PATH_DTYPE),
+        z=np.zeros((m, n + 1), dtype=np.complex128),
+        x=np.zeros((m, nn), dtype=np.complex128),
+        sols=np.zeros((m, nn), dtype=np.complex128),
+        realsols=np.zeros((m, nn)),
+        ssols=np.zeros((m, nn), dtype=np.complex128),
+        mult=np.zeros(m, dtype=np.int32),
+    )
+    rc = _abi.SolveResultC()
+    rc.paths = bufs["paths"].ctypes.data_as(ctypes.c_void_p)
+    rc.z = _abi.dptr(bufs["z"].view(np.float64))
+    rc.x = _abi.dptr(bufs["x"].view(np.float64))
+    rc.solutions = _abi.dptr(bufs["sols"].view(np.float64))
+    rc.real_solutions = _abi.dptr(bufs["realsols"])
+    rc.singular_solutions = _abi.dptr(bufs["ssols"].view(np.float64))
+    rc.multiplicities = _abi.iptr(bufs["mult"])
+    return bufs, rc
+
+
+def _fill_result(n, npaths, bufs, rc):
+    c = rc.counts
+    res = SolveResult()
+    res.n = c.n
+    res.npaths = c.npaths
+    res.paths = bufs["paths"][:npaths]
+    res.z = bufs["z"][:npaths]
+    res.x = bufs["x"][:npaths, :n]
+    res.nsolutions = c.nsolutions
+    res.solutions = bufs["sols"][:c.nsolutions, :n]
+    res.nreal = c.nreal
+    res.real_solutions = bufs["realsols"][:c.nreal, :n]
+    res.nsingular = c.nsingular
+    res.singular_solutions = bufs["ssols"][:c.nsingular, :n]
+    res.multiplicities = bufs["mult"][:c.nsingular]
+    res.ninfinite = c.ninfinite
+    res.nfailed = c.nfailed
+    res.nduplicates = c.nduplicates
+    return res
+
+
+def solve(sys, options=None, gpu=None):
+    """solve(sys, res, status, options), src/solve.f90:154-215, on the GPU.
+    Returns (res, status); status is err_invalid_input for systems the
+    reference rejects. Device errors raise PhcError."""
+    L = _abi.lib()
+    o = options if options is not None else default_options()
+    g = gpu if gpu is not None else default_gpu_options()
+    t, st = sys.table()
+    if st != PHC_OK:
+        return SolveResult(), st
+    n = sys.nvars()
+    npaths = int(L.phc_bezout(ctypes.byref(t)))
+    if npaths < 1:
+        return SolveResult(), ERR_INVALID_INPUT
+    bufs, rc = _result_buffers(n, npaths)
+    st = L.phc_solve_sparse(ctypes.byref(t), ctypes.byref(o), ctypes.byref(g), ctypes.byref(rc))
+    _check_device_status(st, "phc_solve_sparse")
+    if st != PHC_OK:
+        return SolveResult(), st
+    return _fill_result(n, npaths, bufs, rc), st
+
+
+def homotopy_init(sys, seed=1):
+    """gen%seed(seed); hom%init(sys, gen, status): returns (gamma, b, patch,
+    nstart, status) as drawn by the reference generator."""
+    L = _abi.lib()
+    t, st = sys.table()
+    if st != PHC_OK:
+        return None, None, None, 0, st
+    n = sys.nvars()
+    g = np.zeros(1, dtype=np.complex128)
+    b = np.zeros(n, dtype=np.complex128)
+    a = np.zeros(n + 1, dtype=np.complex128)
+    ns = ctypes.c_int64(0)
+    st = L.phc_homotopy_init(ctypes.byref(t), int(seed), _abi.dptr(g.view(np.float64)),
+                             _abi.dptr(b.view(np.float64)), _abi.dptr(a.view(np.float64)),
+                             ctypes.byref(ns))
+    return complex(g[0]), b, a, int(ns.value), st
+
+
+def _homotopy_struct(gamma, b, patch):
+    b = np.ascontiguousarray(b, dtype=np.complex128)
+    patch = np.ascontiguousarray(patch, dtype=np.complex128)
+    h = _abi.HomotopyC()
+    h.gamma[0] = complex(gamma).real
+    h.gamma[1] = complex(gamma).imag
+    h.b = _abi.dptr(b.view(np.float64))
+    h.patch = _abi.dptr(patch.view(np.float64))
+    return h, (b, patch)
+
+
+def solve_paths(sys, options=None, gpu=None, k0=1, count=None, seed=None):
+    """Per-path numerics (start_solution + endpoint + classify) for the
+    1-based paths k0 .. k0+count-1. Returns (paths, z, x, status)."""
+    L = _abi.lib()
+    o = options if options is not None else default_options()
+    g = gpu if gpu is not None else default_gpu_options()
+    gamma, b, patch, nstart, st = homotopy_init(sys, o.seed if seed is None else seed)
+    if st != PHC_OK:
+        return None, None, None, st
+    if count is None:
+        count = nstart - k0 + 1
+    n = sys.nvars()
+    t, _ = sys.table()
+    h, keep = _homotopy_struct(gamma, b, patch)
+    paths = np.zeros(max(count, 1), dtype=PATH_DTYPE)
+    z = np.zeros((max(count, 1), n + 1), dtype=np.complex128)
+    x = np.zeros((max(count, 1), n), dtype=np.complex128)
+    st = L.phc_solve_paths(ctypes.byref(t), ctypes.byref(h), ctypes.byref(o), ctypes.byref(g),
+                           int(k0), int(count), paths.ctypes.data_as(ctypes.c_void_p),
+                           _abi.dptr(z.view(np.float64)), _abi.dptr(x.view(np.float64)))
+    _check_device_status(st, "phc_solve_paths")
+    return paths[:count], z[:count], x[:count], st
+
+
+class Plan:
+    """Device-resident plan: the compiled table lives in device memory and
+    launches write device buffers (phc_plan_create / phc_plan_launch)."""
+
+    def __init__(self, sys, options=None, gpu=None, seed=None):
+        self._L = _abi.lib()
+        o = options if options is not None else default_options()
+        g = gpu if gpu is not None else default_gpu_options()
+        gamma, b, patch, nstart, st = homotopy_init(sys, o.seed if seed is None else seed)
+        if st != PHC_OK:
+            raise PhcError(st, "homotopy_init")
+        t, _ = sys.table()
+        h, keep = _homotopy_struct(gamma, b, patch)
+        self.h = ctypes.c_void_p()
+        st = self._L.phc_plan_create(ctypes.byref(t), ctypes.byref(h), ctypes.byref(o),
+                                     ctypes.byref(g), ctypes.byref(self.h))
+        if st != PHC_OK:
+            raise PhcError(st, "phc_plan_create")
+        self.n = sys.nvars()
+        self.npaths = nstart
+
+    def launch(self, k0, count, d_out, d_z, stream=0):
+        st = self._L.phc_plan_launch(self.h, int(k0), int(count), ctypes.c_void_p(d_out),
+                                     ctypes.c_void_p(d_z), ctypes.c_void_p(stream))
+        if st != PHC_OK:
+            raise PhcError(st, "phc_plan_launch")
+
+    def config(self):
+        w, g, s, nm = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._L.phc_plan_config(self.h, ctypes.byref(w), ctypes.byref(g), ctypes.byref(s),
+                                ctypes.byref(nm))
+        return dict(warps_per_block=w.value, grid=g.value, smem=s.value, nm=nm.value)
+
+    def close(self):
+        if self.h:
+            self._L.phc_plan_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def result_from_arrays(n, paths, x, options=None):
+    """Host bookkeeping of solve() (add_solution, add_singular, find,
+    collect_real) applied to per-path records, in path order. Mirrors
+    src/solve.f90:193-213, :330-426; used when paths were produced by a
+    device-resident plan."""
+    o = options if options is not None else default_options()
+    paths = np.array(paths, dtype=PATH_DTYPE, copy=True)
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    res = SolveResult()
+    res.n = n
+    res.npaths = len(paths)
+    res.paths = paths
+
+    def norm_inf(v):
+        return float(np.max(np.abs(v))) if len(v) else 0.0
+
+    def find(v, pts, tol):
+        scale = max(1.0, norm_inf(v))
+        for j, p in enumerate(pts):
+            if norm_inf(v - p) <= tol * scale:
+                return j + 1
+        return 0
+
+    sols, ssols, mult = [], [], []
+    for k in range(len(paths)):
+        p = paths[k]
+        p["solution_index"] = 0
+        p["singular_index"] = 0
+        if p["status"] != PATH_SUCCESS:
+            res.nfailed += 1
+        elif p["at_infinity"]:
+            res.ninfinite += 1
+        elif p["singular"]:
+            j = find(x[k], ssols, o.singular_dedup_tol)
+            if j > 0:
+                mult[j - 1] += 1
+            else:
+                ssols.append(x[k].copy())
+                mult.append(1)
+                j = len(ssols)
+            p["singular_index"] = j
+        else:
+            j = find(x[k], sols, o.dedup_tol)
+            if j > 0:
+                res.nduplicates += 1
+            else:
+                sols.append(x[k].copy())
+                j = len(sols)
+            p["solution_index"] = j
+    res.nsolutions = len(sols)
+    res.solutions = np.array(sols, dtype=np.complex128).reshape(len(sols), n)
+    res.nsingular = len(ssols)
+    res.singular_solutions = np.array(ssols, dtype=np.complex128).reshape(len(ssols), n)
+    res.multiplicities = np.array(mult, dtype=np.int32)
+    reals = [s.real for s in sols
+             if np.max(np.abs(s.imag)) <= o.real_tol * max(1.0, norm_inf(s))]
+    res.nreal = len(reals)
+    res.real_solutions = np.array(reals).reshape(len(reals), n)
+    return res

@@ -1,0 +1,686 @@
+// phc_api.cpp -- C ABI of the B200 path tracker (include/polyhomocont_b200.h).
+//
+// Host side of the drop-in for solve() (src/solve.f90:154-215): the
+// sparse_system builder, the homotopy set-up with the reference generator,
+// device buffers and launches, and the order-dependent bookkeeping of the
+// solve driver. There is no CPU fallback: without a usable CUDA device
+// every entry point that needs one returns PHC_ERR_NO_DEVICE.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "phc_host.h"
+
+namespace phc {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& s) { g_last_error = s; }
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) return PHC_ERR_OOM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorInvalidDevice)
+    return PHC_ERR_NO_DEVICE;
+  return PHC_ERR_CUDA;
+}
+
+#define PHC_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// options
+// ---------------------------------------------------------------------------
+phc_solve_options solve_defaults() {
+  phc_solve_options o;
+  std::memset(&o, 0, sizeof(o));
+  o.tracker.step_init = 0.05;       // src/tracker.f90:60-76
+  o.tracker.step_max = 0.1;
+  o.tracker.step_min = 1.0e-14;
+  o.tracker.corrector_tol = 1.0e-10;
+  o.tracker.corrector_maxit = 3;
+  o.tracker.contraction = 0.5;
+  o.tracker.grow_after = 5;
+  o.tracker.max_steps = 20000;
+  o.endgame.t_start = 0.1;          // src/endgame.f90:75-100
+  o.endgame.nsamples = 8;
+  o.endgame.radius_factor = 0.25;
+  o.endgame.radius_min = 1.0e-13;
+  o.endgame.max_winding = 16;
+  o.endgame.loop_radius = 1.0e-5;
+  o.endgame.winding_agreement = 0.2;
+  o.endgame.tol = 1.0e-11;
+  o.endgame.residual_tol = 1.0e-8;
+  o.endgame.closure_factor = 0.1;
+  o.use_endgame = 1;                // src/solve.f90:63-83
+  o.seed = 1;
+  o.refine_maxit = 5;
+  o.infinity_tol = 1.0e-8;
+  o.singular_cond = 1.0e10;
+  o.real_tol = 1.0e-8;
+  o.dedup_tol = 1.0e-8;
+  o.singular_dedup_tol = 1.0e-6;
+  return o;
+}
+
+phc_gpu_options gpu_defaults() {
+  phc_gpu_options g;
+  std::memset(&g, 0, sizeof(g));
+  g.precision = PHC_PREC_MIXED;
+  g.schedule = PHC_SCHED_PERSISTENT;
+  g.device = 0;
+  g.warps_per_block = 0;
+  g.blocks_per_sm = 0;
+  g.chunk = 1;
+  g.fp64_sticky = -1;
+  return g;
+}
+
+// The reference runs with any option values; on the GPU, values that would
+// make a loop run forever (radius_factor >= 1, no samples per loop, ...)
+// are rejected up front.
+int validate_options(const phc_solve_options* o) {
+  const phc_tracker_options& t = o->tracker;
+  const phc_endgame_options& e = o->endgame;
+  if (!(t.step_min > 0.0) || !(t.step_init > 0.0) || !(t.step_max > 0.0)) return PHC_ERR_INVALID_INPUT;
+  if (t.corrector_maxit < 1 || t.grow_after < 1 || t.max_steps < 0) return PHC_ERR_INVALID_INPUT;
+  if (!(t.corrector_tol >= 0.0)) return PHC_ERR_INVALID_INPUT;
+  if (o->use_endgame) {
+    if (e.nsamples < 1 || e.max_winding < 1) return PHC_ERR_INVALID_INPUT;
+    if (!(e.radius_factor > 0.0 && e.radius_factor < 1.0)) return PHC_ERR_INVALID_INPUT;
+    if (!(e.radius_min > 0.0) || !(e.t_start > 0.0 && e.t_start < 1.0)) return PHC_ERR_INVALID_INPUT;
+  }
+  if (o->refine_maxit < 0) return PHC_ERR_INVALID_INPUT;
+  return PHC_OK;
+}
+
+KOpts make_kopts(const phc_solve_options& so, const phc_gpu_options& g) {
+  KOpts k;
+  std::memset(&k, 0, sizeof(k));
+  k.so = so;
+  k.precision = g.precision;
+  k.fp64_sticky = g.fp64_sticky < 0 ? 4 : g.fp64_sticky;
+  // safety budget of evaluate+LU units per path; far above any path the
+  // reference tracks in practice, it bounds every kernel's run time
+  k.max_units = (int64_t)1 << 24;
+  return k;
+}
+
+// ---------------------------------------------------------------------------
+// reference generator (src/random.f90) and hom%init (src/homotopy.f90:104-149)
+// ---------------------------------------------------------------------------
+namespace {
+struct Rng {
+  int64_t s1 = 1234567, s2 = 7654321;
+  void seed(int seed) {
+    int64_t s = std::llabs((int64_t)seed);
+    s1 = s % (2147483563LL - 1) + 1;
+    s2 = (s * 7919LL + 104729LL) % (2147483399LL - 1) + 1;
+    for (int i = 0; i < 16; ++i) uniform();
+  }
+  double uniform() {
+    s1 = (40014LL * s1) % 2147483563LL;
+    s2 = (40692LL * s2) % 2147483399LL;
+    int64_t z = s1 - s2;
+    if (z < 1) z += 2147483563LL - 1;
+    return (double)z / 2147483563.0;
+  }
+  void unit_complex(double* z) {
+    const double phi = 2.0 * 3.14159265358979323846 * uniform();
+    z[0] = std::cos(phi);
+    z[1] = std::sin(phi);
+  }
+  void normal_complex(double* z) {
+    const double r = std::sqrt(-std::log(uniform()));
+    const double phi = 2.0 * 3.14159265358979323846 * uniform();
+    z[0] = r * std::cos(phi);
+    z[1] = r * std::sin(phi);
+  }
+};
+}  // namespace
+
+int homotopy_init(const phc_system* sys, int seed, HostHomotopy* h) {
+  if (sys == nullptr || sys->n < 1 || sys->deg == nullptr) return PHC_ERR_INVALID_INPUT;
+  const int n = sys->n;
+  int64_t nstart = 1;
+  for (int i = 0; i < n; ++i) {
+    if (sys->deg[i] < 1) return PHC_ERR_INVALID_INPUT;
+    nstart *= sys->deg[i];
+    if (nstart > (int64_t)INT32_MAX) return PHC_ERR_INVALID_INPUT;
+  }
+  Rng g;
+  g.seed(seed);
+  h->nstart = nstart;
+  g.unit_complex(h->gamma);
+  h->b.assign(2 * n, 0.0);
+  for (int i = 0; i < n; ++i) g.unit_complex(&h->b[2 * i]);
+  h->patch.assign(2 * (n + 1), 0.0);
+  for (int i = 0; i <= n; ++i) g.normal_complex(&h->patch[2 * i]);
+  double ss = 0.0;
+  for (int i = 0; i <= n; ++i) {
+    const double a = std::hypot(h->patch[2 * i], h->patch[2 * i + 1]);
+    ss += a * a;
+  }
+  const double nrm = std::sqrt(ss);
+  for (int i = 0; i < 2 * (n + 1); ++i) h->patch[i] = h->patch[i] / nrm;
+  return PHC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch configuration
+// ---------------------------------------------------------------------------
+static int device_smem_optin(int device) {
+  int v = 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
+    return 48 * 1024;
+  return v;
+}
+static int device_sms(int device) {
+  int v = 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 1;
+  return v;
+}
+
+int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, LaunchCfg* cfg) {
+  cfg->nm = pick_nm(hp.N);
+  if (cfg->nm == 0) {
+    set_last_error("more than 32 unknowns");
+    return PHC_ERR_UNSUPPORTED;
+  }
+  cfg->precision = (g.precision == PHC_PREC_MIXED) ? PHC_PREC_MIXED : PHC_PREC_FP64;
+  cfg->persistent = (g.schedule == PHC_SCHED_PERSISTENT) ? 1 : 0;
+  cfg->chunk = g.chunk > 0 ? g.chunk : 1;
+  cfg->ws_bytes = ws_layout(hp.n, hp.S, hp.pw_size, cfg->precision == PHC_PREC_MIXED).bytes;
+  const int plan_bytes = align16((int)hp.bytes.size());
+  const int smax = device_smem_optin(device);
+  int warps = g.warps_per_block > 0 ? g.warps_per_block : 4;
+  warps = std::min(std::max(warps, 1), 8);
+  while (warps > 1 && plan_bytes + warps * cfg->ws_bytes > smax) --warps;
+  if (plan_bytes + warps * cfg->ws_bytes > smax) {
+    set_last_error("system table does not fit in shared memory");
+    return PHC_ERR_UNSUPPORTED;
+  }
+  cfg->warps = warps;
+  cfg->smem = plan_bytes + warps * cfg->ws_bytes;
+  int bps = track_blocks_per_sm(*cfg);
+  if (bps < 1) bps = 1;
+  if (g.blocks_per_sm > 0) bps = std::min(bps, g.blocks_per_sm);
+  cfg->grid = device_sms(device) * bps;
+  return PHC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-device workspace for the synchronous entry points
+// ---------------------------------------------------------------------------
+namespace {
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t need) {
+    if (need <= cap) return PHC_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(need, (size_t)4096);
+    want += want / 2;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    cap = want;
+    return PHC_OK;
+  }
+};
+struct DeviceWS {
+  std::mutex mu;
+  bool ready = false;
+  cudaStream_t stream = nullptr;
+  DevBuf plan, out, z, x, counter;
+};
+DeviceWS g_ws[64];
+
+int check_device(int device) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count < 1) {
+    set_last_error(e != cudaSuccess ? cudaGetErrorString(e) : "no CUDA device");
+    return PHC_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count || device >= 64) {
+    set_last_error("invalid device ordinal");
+    return PHC_ERR_NO_DEVICE;
+  }
+  return PHC_OK;
+}
+}  // namespace
+
+// Runs paths [k0, k0+count) of a compiled plan on the device workspace and
+// copies the results to host buffers.
+static int run_paths_sync(const HostPlan& hp, const phc_solve_options& so,
+                          const phc_gpu_options& g, int64_t k0, int64_t count,
+                          phc_path_out* out, double* z_out, double* x_out) {
+  int st = check_device(g.device);
+  if (st != PHC_OK) return st;
+  if (count <= 0) return PHC_OK;
+  DeviceWS& W = g_ws[g.device];
+  std::lock_guard<std::mutex> lock(W.mu);
+  PHC_CUDA(cudaSetDevice(g.device));
+  if (!W.ready) {
+    PHC_CUDA(cudaStreamCreateWithFlags(&W.stream, cudaStreamNonBlocking));
+    W.ready = true;
+  }
+  LaunchCfg cfg;
+  st = resolve_launch(hp, g, g.device, &cfg);
+  if (st != PHC_OK) return st;
+  const size_t nout = (size_t)count * sizeof(phc_path_out);
+  const size_t nz = (size_t)count * hp.N * 2 * sizeof(double);
+  const size_t nx = (size_t)count * hp.n * 2 * sizeof(double);
+  if ((st = W.plan.ensure(hp.bytes.size() + 16)) != PHC_OK) return st;
+  if ((st = W.out.ensure(nout)) != PHC_OK) return st;
+  if ((st = W.z.ensure(nz)) != PHC_OK) return st;
+  if ((st = W.x.ensure(nx)) != PHC_OK) return st;
+  if ((st = W.counter.ensure(16)) != PHC_OK) return st;
+  PHC_CUDA(cudaMemcpyAsync(W.plan.p, hp.bytes.data(), hp.bytes.size(), cudaMemcpyHostToDevice,
+                           W.stream));
+  KParams kp;
+  std::memset(&kp, 0, sizeof(kp));
+  kp.plan = static_cast<const unsigned char*>(W.plan.p);
+  kp.plan_bytes = align16((int)hp.bytes.size());
+  kp.ws_bytes = cfg.ws_bytes;
+  kp.warps = cfg.warps;
+  kp.persistent = cfg.persistent;
+  kp.chunk = cfg.chunk;
+  kp.k0 = k0;
+  kp.count = count;
+  kp.counter = static_cast<unsigned long long*>(W.counter.p);
+  kp.out = static_cast<phc_path_out*>(W.out.p);
+  kp.z = static_cast<double*>(W.z.p);
+  kp.x = static_cast<double*>(W.x.p);
+  kp.opts = make_kopts(so, g);
+  int grid;
+  if (cfg.persistent) {
+    PHC_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned long long), W.stream));
+    const int64_t need = (count + (int64_t)cfg.warps * cfg.chunk - 1) / ((int64_t)cfg.warps * cfg.chunk);
+    grid = (int)std::min<int64_t>(cfg.grid, need);
+  } else {
+    grid = (int)((count + cfg.warps - 1) / cfg.warps);
+  }
+  cudaError_t e = launch_track(cfg, kp, grid, W.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "track kernel launch");
+  PHC_CUDA(cudaMemcpyAsync(out, W.out.p, nout, cudaMemcpyDeviceToHost, W.stream));
+  PHC_CUDA(cudaMemcpyAsync(z_out, W.z.p, nz, cudaMemcpyDeviceToHost, W.stream));
+  if (x_out) PHC_CUDA(cudaMemcpyAsync(x_out, W.x.p, nx, cudaMemcpyDeviceToHost, W.stream));
+  PHC_CUDA(cudaStreamSynchronize(W.stream));
+  return PHC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// bookkeeping (src/solve.f90:193-213, :330-426)
+// ---------------------------------------------------------------------------
+static double norm_inf_c(const double* v, int n) {
+  double r = 0.0;
+  for (int i = 0; i < n; ++i) r = std::max(r, std::hypot(v[2 * i], v[2 * i + 1]));
+  return r;
+}
+
+// find(x, pts, tol): first stored point within relative distance tol
+static int find_first(const double* x, const std::vector<double>& pts, int npts, int n,
+                      double tol) {
+  const double scale = std::max(1.0, norm_inf_c(x, n));
+  for (int j = 0; j < npts; ++j) {
+    const double* p = pts.data() + (size_t)j * 2 * n;
+    double d = 0.0;
+    for (int i = 0; i < n; ++i)
+      d = std::max(d, std::hypot(x[2 * i] - p[2 * i], x[2 * i + 1] - p[2 * i + 1]));
+    if (d <= tol * scale) return j + 1;
+  }
+  return 0;
+}
+
+void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out* paths,
+                 const double* x, phc_solve_result* res) {
+  phc_solve_counts& c = res->counts;
+  std::vector<double> sols, ssols;
+  std::vector<int> mult;
+  int nsol = 0, nsing = 0;
+  for (int64_t k = 0; k < npaths; ++k) {
+    phc_path_out& p = paths[k];
+    const double* xk = x + (size_t)k * 2 * n;
+    p.solution_index = 0;
+    p.singular_index = 0;
+    if (p.status != PHC_PATH_SUCCESS) {
+      c.nfailed++;
+    } else if (p.at_infinity) {
+      c.ninfinite++;
+    } else if (p.singular) {
+      int j = find_first(xk, ssols, nsing, n, o.singular_dedup_tol);
+      if (j > 0) {
+        mult[j - 1]++;
+      } else {
+        ssols.insert(ssols.end(), xk, xk + 2 * n);
+        mult.push_back(1);
+        j = ++nsing;
+      }
+      p.singular_index = j;
+    } else {
+      int j = find_first(xk, sols, nsol, n, o.dedup_tol);
+      if (j > 0) {
+        c.nduplicates++;
+      } else {
+        sols.insert(sols.end(), xk, xk + 2 * n);
+        j = ++nsol;
+      }
+      p.solution_index = j;
+    }
+  }
+  c.nsolutions = nsol;
+  c.nsingular = nsing;
+  if (res->solutions && nsol) std::memcpy(res->solutions, sols.data(), sols.size() * sizeof(double));
+  if (res->singular_solutions && nsing)
+    std::memcpy(res->singular_solutions, ssols.data(), ssols.size() * sizeof(double));
+  if (res->multiplicities)
+    for (int j = 0; j < nsing; ++j) res->multiplicities[j] = mult[j];
+  // collect_real, src/solve.f90:402-426
+  int nreal = 0;
+  for (int j = 0; j < nsol; ++j) {
+    const double* s = sols.data() + (size_t)j * 2 * n;
+    double imax = 0.0;
+    for (int i = 0; i < n; ++i) imax = std::max(imax, std::fabs(s[2 * i + 1]));
+    if (imax <= o.real_tol * std::max(1.0, norm_inf_c(s, n))) {
+      if (res->real_solutions)
+        for (int i = 0; i < n; ++i) res->real_solutions[(size_t)nreal * n + i] = s[2 * i];
+      ++nreal;
+    }
+  }
+  c.nreal = nreal;
+}
+
+}  // namespace phc
+
+// ---------------------------------------------------------------------------
+// type(sparse_system) builder
+// ---------------------------------------------------------------------------
+struct phc_sparse {
+  int n = 0;
+  int neq = 0;
+  bool initialized = false;
+  std::vector<int32_t> first;  // 0-based, neq + 1
+  std::vector<int32_t> deg;
+  std::vector<int32_t> hexps;  // term-major [nt][n+1]
+  std::vector<double> coefs;   // [nt][2]
+};
+
+using namespace phc;
+
+extern "C" {
+
+const char* phc_version(void) { return "polyhomocont_b200 0.1.0 (sm_100a)"; }
+const char* phc_last_error(void) { return g_last_error.c_str(); }
+
+void phc_default_solve_options(phc_solve_options* o) {
+  if (o) *o = solve_defaults();
+}
+void phc_default_gpu_options(phc_gpu_options* g) {
+  if (g) *g = gpu_defaults();
+}
+
+phc_sparse* phc_sparse_create(void) { return new (std::nothrow) phc_sparse(); }
+void phc_sparse_destroy(phc_sparse* s) { delete s; }
+
+int32_t phc_sparse_init(phc_sparse* s, int32_t n) {  // src/sparse.f90:65-81
+  if (!s) return PHC_ERR_BAD_HANDLE;
+  s->n = n;
+  s->neq = 0;
+  s->initialized = true;
+  s->first.assign(1, 0);
+  s->deg.clear();
+  s->hexps.clear();
+  s->coefs.clear();
+  return PHC_OK;
+}
+
+int32_t phc_sparse_add_equation(phc_sparse* s, int32_t ncoefs, const double* coefs,
+                                int32_t rows, int32_t cols, const int32_t* exps) {
+  // src/sparse.f90:83-141: validation, zero terms dropped, degree from the
+  // kept terms, homogenized exponent of w = d - |a|
+  if (!s || !s->initialized) return PHC_ERR_INVALID_INPUT;
+  if (s->neq >= s->n) return PHC_ERR_INVALID_INPUT;
+  if (rows != s->n) return PHC_ERR_INVALID_INPUT;
+  if (cols != ncoefs || ncoefs < 0) return PHC_ERR_INVALID_INPUT;
+  if (ncoefs > 0 && (coefs == nullptr || exps == nullptr)) return PHC_ERR_INVALID_INPUT;
+  for (int64_t q = 0; q < (int64_t)rows * cols; ++q)
+    if (exps[q] < 0) return PHC_ERR_INVALID_INPUT;
+  int d = 0;
+  for (int k = 0; k < ncoefs; ++k) {
+    if (coefs[2 * k] == 0.0 && coefs[2 * k + 1] == 0.0) continue;
+    int sum = 0;
+    for (int j = 0; j < rows; ++j) sum += exps[(size_t)k * rows + j];
+    d = std::max(d, sum);
+  }
+  if (d < 1) return PHC_ERR_INVALID_INPUT;
+  int kept = 0;
+  for (int k = 0; k < ncoefs; ++k) {
+    if (coefs[2 * k] == 0.0 && coefs[2 * k + 1] == 0.0) continue;
+    int sum = 0;
+    for (int j = 0; j < rows; ++j) {
+      const int e = exps[(size_t)k * rows + j];
+      s->hexps.push_back(e);
+      sum += e;
+    }
+    s->hexps.push_back(d - sum);
+    s->coefs.push_back(coefs[2 * k]);
+    s->coefs.push_back(coefs[2 * k + 1]);
+    ++kept;
+  }
+  s->neq += 1;
+  s->first.push_back(s->first.back() + kept);
+  s->deg.push_back(d);
+  return PHC_OK;
+}
+
+int32_t phc_sparse_nvars(const phc_sparse* s) { return s ? s->n : 0; }
+int32_t phc_sparse_nequations(const phc_sparse* s) { return s ? s->neq : 0; }
+int32_t phc_sparse_nterms(const phc_sparse* s, int32_t i) {
+  if (!s || i < 1 || i > s->neq) return 0;
+  return s->first[i] - s->first[i - 1];
+}
+int32_t phc_sparse_total_terms(const phc_sparse* s) { return s ? (int32_t)(s->coefs.size() / 2) : 0; }
+void phc_sparse_degrees(const phc_sparse* s, int32_t* d) {
+  if (!s || !d) return;
+  for (int i = 0; i < s->neq; ++i) d[i] = s->deg[i];
+}
+int32_t phc_sparse_table(const phc_sparse* s, phc_system* out) {
+  if (!s || !out) return PHC_ERR_BAD_HANDLE;
+  out->n = s->n;
+  out->nterms = (int32_t)(s->coefs.size() / 2);
+  out->first = s->first.data();
+  out->deg = s->deg.data();
+  out->hexps = s->hexps.data();
+  out->coefs = s->coefs.data();
+  // hom%init rejects systems whose equation count differs from n
+  // (src/homotopy.f90:106-108)
+  return (s->neq == s->n && s->n >= 1) ? PHC_OK : PHC_ERR_INVALID_INPUT;
+}
+
+int32_t phc_homotopy_init(const phc_system* sys, int32_t seed, double* gamma, double* b,
+                          double* patch, int64_t* nstart) {
+  HostHomotopy h;
+  int st = homotopy_init(sys, seed, &h);
+  if (st != PHC_OK) return st;
+  if (gamma) {
+    gamma[0] = h.gamma[0];
+    gamma[1] = h.gamma[1];
+  }
+  if (b) std::memcpy(b, h.b.data(), h.b.size() * sizeof(double));
+  if (patch) std::memcpy(patch, h.patch.data(), h.patch.size() * sizeof(double));
+  if (nstart) *nstart = h.nstart;
+  return PHC_OK;
+}
+
+int64_t phc_bezout(const phc_system* sys) {
+  if (!sys || sys->n < 1 || !sys->deg) return 0;
+  int64_t b = 1;
+  for (int i = 0; i < sys->n; ++i) {
+    if (sys->deg[i] < 1) return 0;
+    b *= sys->deg[i];
+    if (b > (int64_t)INT32_MAX) return 0;
+  }
+  return b;
+}
+
+int32_t phc_solve_paths(const phc_system* sys, const phc_homotopy* hom,
+                        const phc_solve_options* opts, const phc_gpu_options* gpu,
+                        int64_t k0, int64_t count, phc_path_out* out, double* z_out,
+                        double* x_out) {
+  const phc_solve_options so = opts ? *opts : solve_defaults();
+  const phc_gpu_options g = gpu ? *gpu : gpu_defaults();
+  int st = validate_options(&so);
+  if (st != PHC_OK) return st;
+  if (!out || !z_out || count < 0 || k0 < 1) return PHC_ERR_INVALID_INPUT;
+  HostPlan hp;
+  st = build_plan(sys, hom, &hp);
+  if (st != PHC_OK) return st;
+  if (k0 + count - 1 > hp.nstart) return PHC_ERR_INVALID_INPUT;
+  return run_paths_sync(hp, so, g, k0, count, out, z_out, x_out);
+}
+
+int32_t phc_solve_sparse(const phc_system* sys, const phc_solve_options* opts,
+                         const phc_gpu_options* gpu, phc_solve_result* res) {
+  // solve(sys, res, status, options), src/solve.f90:154-215
+  const phc_solve_options so = opts ? *opts : solve_defaults();
+  const phc_gpu_options g = gpu ? *gpu : gpu_defaults();
+  if (!res) return PHC_ERR_INVALID_INPUT;
+  std::memset(&res->counts, 0, sizeof(res->counts));
+  int st = validate_options(&so);
+  if (st != PHC_OK) return st;
+  st = validate_system(sys);
+  if (st != PHC_OK) return st;
+  HostHomotopy h;
+  st = homotopy_init(sys, so.seed, &h);  // gen%seed + hom%init
+  if (st != PHC_OK) return st;
+  if (!res->paths || !res->z || !res->x) return PHC_ERR_INVALID_INPUT;
+  const phc_homotopy hv = h.view();
+  HostPlan hp;
+  st = build_plan(sys, &hv, &hp);
+  if (st != PHC_OK) return st;
+  st = run_paths_sync(hp, so, g, 1, h.nstart, res->paths, res->z, res->x);
+  if (st != PHC_OK) return st;
+  res->counts.n = sys->n;
+  res->counts.npaths = (int32_t)h.nstart;
+  bookkeeping(sys->n, h.nstart, so, res->paths, res->x, res);
+  return PHC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// device-resident plans
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct phc_plan {
+  int device = 0;
+  HostPlan hp;
+  LaunchCfg cfg;
+  KOpts kopts;
+  void* d_plan = nullptr;
+  unsigned long long* d_counter = nullptr;
+};
+
+extern "C" {
+
+int32_t phc_plan_create(const phc_system* sys, const phc_homotopy* hom,
+                        const phc_solve_options* opts, const phc_gpu_options* gpu,
+                        phc_plan** plan) {
+  if (!plan) return PHC_ERR_INVALID_INPUT;
+  *plan = nullptr;
+  const phc_solve_options so = opts ? *opts : solve_defaults();
+  const phc_gpu_options g = gpu ? *gpu : gpu_defaults();
+  int st = validate_options(&so);
+  if (st != PHC_OK) return st;
+  st = check_device(g.device);
+  if (st != PHC_OK) return st;
+  std::unique_ptr<phc_plan> p(new (std::nothrow) phc_plan());
+  if (!p) return PHC_ERR_OOM;
+  st = build_plan(sys, hom, &p->hp);
+  if (st != PHC_OK) return st;
+  p->device = g.device;
+  PHC_CUDA(cudaSetDevice(g.device));
+  st = resolve_launch(p->hp, g, g.device, &p->cfg);
+  if (st != PHC_OK) return st;
+  p->kopts = make_kopts(so, g);
+  PHC_CUDA(cudaMalloc(&p->d_plan, p->hp.bytes.size() + 16));
+  PHC_CUDA(cudaMalloc((void**)&p->d_counter, 16));
+  PHC_CUDA(cudaMemcpy(p->d_plan, p->hp.bytes.data(), p->hp.bytes.size(), cudaMemcpyHostToDevice));
+  *plan = p.release();
+  return PHC_OK;
+}
+
+int32_t phc_plan_launch(phc_plan* p, int64_t k0, int64_t count, phc_path_out* d_out,
+                        double* d_z, void* stream) {
+  if (!p) return PHC_ERR_BAD_HANDLE;
+  if (count <= 0) return PHC_OK;
+  if (k0 < 1 || k0 + count - 1 > p->hp.nstart || !d_out || !d_z) return PHC_ERR_INVALID_INPUT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PHC_CUDA(cudaSetDevice(p->device));
+  KParams kp;
+  std::memset(&kp, 0, sizeof(kp));
+  kp.plan = static_cast<const unsigned char*>(p->d_plan);
+  kp.plan_bytes = align16((int)p->hp.bytes.size());
+  kp.ws_bytes = p->cfg.ws_bytes;
+  kp.warps = p->cfg.warps;
+  kp.persistent = p->cfg.persistent;
+  kp.chunk = p->cfg.chunk;
+  kp.k0 = k0;
+  kp.count = count;
+  kp.counter = p->d_counter;
+  kp.out = d_out;
+  kp.z = d_z;
+  kp.x = nullptr;
+  kp.opts = p->kopts;
+  int grid;
+  if (p->cfg.persistent) {
+    PHC_CUDA(cudaMemsetAsync(p->d_counter, 0, sizeof(unsigned long long), s));
+    const int64_t per = (int64_t)p->cfg.warps * p->cfg.chunk;
+    grid = (int)std::min<int64_t>(p->cfg.grid, (count + per - 1) / per);
+  } else {
+    grid = (int)((count + p->cfg.warps - 1) / p->cfg.warps);
+  }
+  cudaError_t e = launch_track(p->cfg, kp, grid, s);
+  if (e != cudaSuccess) return cuda_fail(e, "track kernel launch");
+  return PHC_OK;
+}
+
+int32_t phc_plan_launch_count(const phc_plan* p) { return p ? 1 : 0; }
+
+int32_t phc_plan_config(const phc_plan* p, int32_t* warps, int32_t* grid, int32_t* smem,
+                        int32_t* nm) {
+  if (!p) return PHC_ERR_BAD_HANDLE;
+  if (warps) *warps = p->cfg.warps;
+  if (grid) *grid = p->cfg.grid;
+  if (smem) *smem = p->cfg.smem;
+  if (nm) *nm = p->cfg.nm;
+  return PHC_OK;
+}
+
+int32_t phc_plan_destroy(phc_plan* p) {
+  if (!p) return PHC_ERR_BAD_HANDLE;
+  cudaSetDevice(p->device);
+  if (p->d_plan) cudaFree(p->d_plan);
+  if (p->d_counter) cudaFree(p->d_counter);
+  delete p;
+  return PHC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+// phc_host.h -- host-side internals shared by the C ABI implementation,
+// the plan builder, the kernel launcher and the serving loop.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "phc_internal.h"
+#include "polyhomocont_b200.h"
+
+namespace phc {
+
+struct HostPlan {
+  std::vector<unsigned char> bytes;  // PlanHeader + records
+  int n = 0, N = 0, S = 0, maxexp = 0, pw_size = 0, nrec = 0;
+  int64_t nstart = 0;
+};
+
+int validate_system(const phc_system* sys);
+int validate_options(const phc_solve_options* o);
+int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out);
+
+// Homotopy constants drawn on the host with the reference generator.
+struct HostHomotopy {
+  double gamma[2] = {1.0, 0.0};
+  std::vector<double> b, patch;
+  int64_t nstart = 0;
+  phc_homotopy view() const {
+    phc_homotopy h;
+    h.gamma[0] = gamma[0];
+    h.gamma[1] = gamma[1];
+    h.b = b.data();
+    h.patch = patch.data();
+    return h;
+  }
+};
+int homotopy_init(const phc_system* sys, int seed, HostHomotopy* h);
+
+// Launch configuration resolved for a plan.
+struct LaunchCfg {
+  int nm = 0;          // register-row capacity
+  int precision = 0;   // PHC_PREC_*
+  int warps = 4;       // warps per block
+  int persistent = 0;
+  int chunk = 1;
+  int grid = 0;        // persistent grid (blocks)
+  int ws_bytes = 0;
+  int smem = 0;        // dynamic shared memory per block
+};
+
+// Resolves the launch configuration for a plan on a device.
+int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, LaunchCfg* cfg);
+// Launches the tracking kernel (phc_kernels.cu).
+cudaError_t launch_track(const LaunchCfg& cfg, const KParams& kp, int grid, cudaStream_t s);
+// Occupancy (blocks per SM) of the kernel for a configuration.
+int track_blocks_per_sm(const LaunchCfg& cfg);
+
+KOpts make_kopts(const phc_solve_options& so, const phc_gpu_options& g);
+phc_gpu_options gpu_defaults();
+phc_solve_options solve_defaults();
+
+void set_last_error(const std::string& s);
+int cuda_fail(cudaError_t e, const char* what);
+
+// Host bookkeeping of solve() (add_solution, add_singular, find,
+// collect_real; src/solve.f90:193-213, :330-426), in path order.
+void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out* paths,
+                 const double* x, phc_solve_result* res);
+
+}  // namespace phc

@@ -1,0 +1,157 @@
+// phc_internal.h -- layout of the device-side system table ("plan") and
+// of the kernel parameters, shared by the host plan builder
+// (phc_plan.cpp) and the CUDA kernels (phc_kernels.cu).
+//
+// The reference evaluates F^h and its Jacobian per term with prefix and
+// suffix products over all N variables (eval_terms, src/sparse.f90:223-280).
+// Here the table is compiled once per system into "contributions": one
+// record per (output entry, term) pair, i.e. the value c*z^a of a term for
+// f_i and the partial derivative c*e_j*z_j^(e_j-1)*prod_{l!=j} z_l^(e_l) for
+// J(i,j), each as a coefficient times a short list of power-table factors.
+// Output entries are assigned to the 32 lanes of a warp by a
+// longest-processing-time schedule; each lane sums the contributions of
+// its entries in the reference's term order and writes the sum once, so
+// no two lanes touch the same entry and the result is deterministic.
+#pragma once
+
+#include <cstdint>
+
+#include "polyhomocont_b200.h"
+
+#if defined(__CUDACC__)
+#define PHC_HD __host__ __device__
+#else
+#define PHC_HD
+#endif
+
+namespace phc {
+
+constexpr int kMaxN = 32;      // unknowns N = n + 1 (one lane per row)
+constexpr int kMaxFac = 6;     // power-table factors per record
+constexpr int kMaxPw = 1024;   // power-table entries (maxexp + 1) * N
+constexpr int kWarp = 32;
+
+enum : uint8_t {
+  kRecLast = 1,     // last contribution of its entry: store the sum
+  kRecContIn = 2,   // continues the product of the previous record
+  kRecContOut = 4,  // product continues in the next record
+};
+
+// One contribution: coef * prod_{q < nf} pw[fac[q]], pw[e*N + j] = z_j^e.
+struct alignas(16) Rec {
+  double cre;
+  double cim;
+  uint16_t dest;   // f: equation i; J: i*S + j (row-major, odd stride S)
+  uint8_t nf;
+  uint8_t flags;
+  uint16_t fac[kMaxFac];
+};
+static_assert(sizeof(Rec) == 32, "record must be 32 bytes");
+
+struct alignas(16) PlanHeader {
+  int32_t n;            // variables / equations
+  int32_t N;            // unknowns n + 1
+  int32_t S;            // row stride of the Jacobian buffer (odd)
+  int32_t maxexp;       // largest homogenized exponent
+  int32_t pw_size;      // (maxexp + 1) * N
+  int32_t nrec_f;       // records of the f schedule
+  int32_t nrec_j;       // records of the Jacobian schedule
+  int32_t total_bytes;  // header + records (multiple of 16)
+  int32_t lane_f[kWarp + 1];
+  int32_t lane_j[kWarp + 1];
+  int32_t deg[kMaxN];
+  int32_t pad0_[2];
+  int64_t radix[kMaxN];     // prod_{l < i} d_l (mixed-radix start index)
+  int64_t nstart;           // Bezout number
+  int64_t pad1_;
+  double argb[kMaxN];       // atan2(Im b_i, Re b_i), host libm
+  double gamma[2];
+  double b[kMaxN][2];
+  double patch[kMaxN][2];
+};
+
+// Per-kernel options: the POD mirror of solve_options plus GPU knobs.
+struct KOpts {
+  phc_solve_options so;
+  int32_t precision;     // PHC_PREC_*
+  int32_t fp64_sticky;   // mixed: FP64 step attempts after an FP32 failure
+  int64_t max_units;     // safety budget of units per path
+};
+
+struct KParams {
+  const unsigned char* plan;  // device copy of header + records
+  int32_t plan_bytes;
+  int32_t ws_bytes;           // per-warp workspace bytes
+  int32_t warps;              // warps per block
+  int32_t persistent;         // 1: atomic queue, 0: one path per warp
+  int32_t chunk;              // paths per queue grab
+  int32_t pad_;
+  int64_t k0;                 // first path (1-based)
+  int64_t count;              // number of paths
+  unsigned long long* counter;  // persistent queue head (device)
+  phc_path_out* out;          // [count]
+  double* z;                  // [count][N][2]
+  double* x;                  // [count][n][2] or null
+  KOpts opts;
+};
+
+// Cold per-path state of the tracker state machine, kept in shared memory
+// (one per warp) so that registers stay free for the evaluation and the LU.
+// Scalars are warp-uniform; the vectors hold component j in slot j.
+struct alignas(16) WarpState {
+  double zold[kWarp][2];   // end game: z before a radial segment
+  double est[kWarp][2];    // current Cauchy estimate
+  double prev[kWarp][2];   // previous estimate
+  double resz[kWarp][2];   // best estimate so far (res%z)
+  double zprev[kWarp][2];  // loops: point before the last arc
+  double zsum[kWarp][2];   // loops: sum of the samples
+  double hsave[kWarp][2];  // classify: H(z, 0) of the last evaluation
+  double xv[kWarp][2];     // classify: affine endpoint z(1:n)/w
+  double seg_t0[2], seg_t1[2];
+  double seg_r, seg_th0, seg_dth;
+  double o_step_init, o_step_max;
+  double p_t, p_ege, p_cond, p_resid;
+  double r, rnew, best_resid, dprev, cest, cest_prev, eg_segstep, eg_error, eg_residual,
+      eg_radius, rec_err;
+  double lp_spacing, lp_floor, lp_dth;
+  long long units;
+  int seg_arc, o_grow, seg_cont;
+  int p_status, p_wind, p_egs, p_nacc, p_nrej, p_atinf, p_sing, p_real;
+  int c_tan, c_new, c_ref, c_eval, c_cond, c_retry;
+  int max_loops, eg_status, eg_wind, eg_nacc, eg_nrej, cw, rec_cont, have_prev, gate;
+  int lp_c, lp_j, lp_max, lp_nsamp, lp_cont, lp_ok;
+  int rf_it, sticky;
+};
+
+// Per-warp shared-memory workspace layout (byte offsets from the warp's
+// base), shared by host (sizing) and device (addressing).
+struct WsLayout {
+  int pwd, pwf, fvd, fvf, jd, jf, prow, st, bytes;
+};
+
+PHC_HD inline int align16(int x) { return (x + 15) & ~15; }
+
+PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size, bool mixed) {
+  WsLayout L;
+  int off = 0;
+  L.pwd = off; off += align16(pw_size * 16);
+  L.pwf = off; off += mixed ? align16(pw_size * 8) : 0;
+  L.fvd = off; off += kWarp * 16;
+  L.fvf = off; off += mixed ? kWarp * 8 : 0;
+  L.jd = off; off += align16(n * S * 16);
+  L.jf = off; off += mixed ? align16(n * S * 8) : 0;
+  L.prow = off; off += kWarp * 16;
+  L.st = off; off += align16((int)sizeof(WarpState));
+  L.bytes = off;
+  return L;
+}
+
+// Supported register-row widths (compile-time N capacity).
+constexpr int kNMs[] = {6, 8, 12, 16, 18, 24, 32};
+inline int pick_nm(int N) {
+  for (int v : kNMs)
+    if (N <= v) return v;
+  return 0;
+}
+
+}  // namespace phc

@@ -1,0 +1,488 @@
+// phc_server.cpp -- serving loop with continuous batching.
+//
+// Requests are whole solve() calls (a sparse system plus solve_options).
+// An engine thread admits pending requests into batches as soon as a slot
+// (a CUDA stream with its device and pinned buffers) and enough of the
+// device-memory budget are free, launches the batch while other batches
+// are still running, and finishes each request on the host (bookkeeping,
+// src/solve.f90:193-213) when its batch's event has fired. Requests that
+// arrive while the GPU is busy therefore start as soon as any slot frees
+// up, and the work of different batches overlaps on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "phc_host.h"
+
+namespace phc {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  uint64_t ticket = 0;
+  // owned copy of the system table and options
+  int n = 0;
+  std::vector<int32_t> first, deg, hexps;
+  std::vector<double> coefs;
+  phc_solve_options opts;
+  HostHomotopy hom;
+  HostPlan plan;
+  int64_t npaths = 0;
+  size_t dev_bytes = 0;
+  int status = PHC_OK;
+  // results
+  std::vector<phc_path_out> paths;
+  std::vector<double> z, x, sols, realsols, ssols;
+  std::vector<int32_t> mult;
+  phc_solve_counts counts;
+  Clock::time_point t_submit, t_done;
+  bool done = false;
+  // placement inside a batch
+  size_t off_plan = 0, off_out = 0, off_z = 0, off_x = 0;
+  LaunchCfg cfg;
+
+  phc_system view() const {
+    phc_system s;
+    s.n = n;
+    s.nterms = (int32_t)(coefs.size() / 2);
+    s.first = first.data();
+    s.deg = deg.data();
+    s.hexps = hexps.data();
+    s.coefs = coefs.data();
+    return s;
+  }
+};
+
+struct Slot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  void* dbuf = nullptr;
+  size_t dcap = 0;
+  unsigned char* hbuf = nullptr;  // pinned: plans in, results out
+  size_t hcap = 0;
+  unsigned long long* counters = nullptr;  // one queue head per request
+  size_t ccap = 0;
+  std::vector<std::shared_ptr<Request>> batch;
+  size_t bytes = 0;
+  bool busy = false;
+};
+
+inline size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+}  // namespace phc
+
+using namespace phc;
+
+struct phc_server {
+  phc_server_config cfg;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<std::shared_ptr<Request>> pending;
+  std::map<uint64_t, std::shared_ptr<Request>> all;
+  std::vector<Slot> slots;
+  std::thread engine;
+  bool stop = false;
+  uint64_t next_ticket = 1;
+  int64_t submitted = 0, completed = 0, batches = 0;
+  size_t mem_in_use = 0;
+  int init_status = PHC_OK;
+};
+
+namespace phc {
+namespace {
+
+// Lays out a batch in one device buffer and one pinned buffer:
+// [plans | outputs(paths) | z | x], each request's region 256-aligned.
+size_t layout_batch(std::vector<std::shared_ptr<Request>>& b) {
+  size_t off = 0;
+  for (auto& r : b) {
+    r->off_plan = off;
+    off += up256(r->plan.bytes.size());
+  }
+  for (auto& r : b) {
+    r->off_out = off;
+    off += up256((size_t)r->npaths * sizeof(phc_path_out));
+    r->off_z = off;
+    off += up256((size_t)r->npaths * (r->n + 1) * 16);
+    r->off_x = off;
+    off += up256((size_t)r->npaths * r->n * 16);
+  }
+  return off;
+}
+
+int grow(Slot& s, size_t bytes, size_t ncounters) {
+  if (bytes > s.dcap) {
+    if (s.dbuf) cudaFree(s.dbuf);
+    s.dbuf = nullptr;
+    s.dcap = 0;
+    cudaError_t e = cudaMalloc(&s.dbuf, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "server cudaMalloc");
+    s.dcap = bytes;
+  }
+  if (bytes > s.hcap) {
+    if (s.hbuf) cudaFreeHost(s.hbuf);
+    s.hbuf = nullptr;
+    s.hcap = 0;
+    cudaError_t e = cudaMallocHost((void**)&s.hbuf, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "server cudaMallocHost");
+    s.hcap = bytes;
+  }
+  if (ncounters > s.ccap) {
+    if (s.counters) cudaFree(s.counters);
+    s.counters = nullptr;
+    s.ccap = 0;
+    cudaError_t e = cudaMalloc((void**)&s.counters, ncounters * sizeof(unsigned long long));
+    if (e != cudaSuccess) return cuda_fail(e, "server counters");
+    s.ccap = ncounters;
+  }
+  return PHC_OK;
+}
+
+int launch_batch(phc_server* S, Slot& s) {
+  const phc_gpu_options& g = S->cfg.gpu;
+  size_t bytes = layout_batch(s.batch);
+  int st = grow(s, bytes, s.batch.size());
+  if (st != PHC_OK) return st;
+  s.bytes = bytes;
+  unsigned char* dev = static_cast<unsigned char*>(s.dbuf);
+  size_t plan_end = 0;
+  for (auto& r : s.batch) {
+    std::memcpy(s.hbuf + r->off_plan, r->plan.bytes.data(), r->plan.bytes.size());
+    plan_end = std::max(plan_end, r->off_plan + up256(r->plan.bytes.size()));
+  }
+  cudaError_t e = cudaMemcpyAsync(dev, s.hbuf, plan_end, cudaMemcpyHostToDevice, s.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "server H2D");
+  e = cudaMemsetAsync(s.counters, 0, s.batch.size() * sizeof(unsigned long long), s.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "server counters reset");
+  for (size_t i = 0; i < s.batch.size(); ++i) {
+    Request& r = *s.batch[i];
+    KParams kp;
+    std::memset(&kp, 0, sizeof(kp));
+    kp.plan = dev + r.off_plan;
+    kp.plan_bytes = align16((int)r.plan.bytes.size());
+    kp.ws_bytes = r.cfg.ws_bytes;
+    kp.warps = r.cfg.warps;
+    kp.persistent = r.cfg.persistent;
+    kp.chunk = r.cfg.chunk;
+    kp.k0 = 1;
+    kp.count = r.npaths;
+    kp.counter = s.counters + i;
+    kp.out = reinterpret_cast<phc_path_out*>(dev + r.off_out);
+    kp.z = reinterpret_cast<double*>(dev + r.off_z);
+    kp.x = reinterpret_cast<double*>(dev + r.off_x);
+    kp.opts = make_kopts(r.opts, g);
+    int grid;
+    if (r.cfg.persistent) {
+      const int64_t per = (int64_t)r.cfg.warps * r.cfg.chunk;
+      grid = (int)std::min<int64_t>(r.cfg.grid, (r.npaths + per - 1) / per);
+    } else {
+      grid = (int)((r.npaths + r.cfg.warps - 1) / r.cfg.warps);
+    }
+    e = launch_track(r.cfg, kp, grid, s.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "server kernel launch");
+  }
+  // results of the whole batch in one copy
+  size_t res_begin = plan_end;
+  e = cudaMemcpyAsync(s.hbuf + res_begin, dev + res_begin, bytes - res_begin,
+                      cudaMemcpyDeviceToHost, s.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "server D2H");
+  e = cudaEventRecord(s.done, s.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "server event");
+  return PHC_OK;
+}
+
+void finish_request(Request& r, const unsigned char* h) {
+  const int n = r.n;
+  r.paths.resize(r.npaths);
+  std::memcpy(r.paths.data(), h + r.off_out, (size_t)r.npaths * sizeof(phc_path_out));
+  r.z.resize((size_t)r.npaths * (n + 1) * 2);
+  std::memcpy(r.z.data(), h + r.off_z, r.z.size() * sizeof(double));
+  r.x.resize((size_t)r.npaths * n * 2);
+  std::memcpy(r.x.data(), h + r.off_x, r.x.size() * sizeof(double));
+  r.sols.assign((size_t)r.npaths * n * 2, 0.0);
+  r.realsols.assign((size_t)r.npaths * n, 0.0);
+  r.ssols.assign((size_t)r.npaths * n * 2, 0.0);
+  r.mult.assign(r.npaths, 0);
+  phc_solve_result res;
+  std::memset(&res, 0, sizeof(res));
+  res.solutions = r.sols.data();
+  res.real_solutions = r.realsols.data();
+  res.singular_solutions = r.ssols.data();
+  res.multiplicities = r.mult.data();
+  bookkeeping(n, r.npaths, r.opts, r.paths.data(), r.x.data(), &res);
+  r.counts = res.counts;
+  r.counts.n = n;
+  r.counts.npaths = (int32_t)r.npaths;
+}
+
+void engine_main(phc_server* S) {
+  cudaSetDevice(S->cfg.device);
+  const int64_t max_paths = S->cfg.max_batch_paths > 0 ? S->cfg.max_batch_paths : (1 << 20);
+  const int max_sys = S->cfg.max_batch_systems > 0 ? S->cfg.max_batch_systems : 256;
+  std::unique_lock<std::mutex> lk(S->mu);
+  for (;;) {
+    bool progressed = false;
+    // 1. completions
+    for (auto& s : S->slots) {
+      if (!s.busy) continue;
+      if (cudaEventQuery(s.done) != cudaSuccess) continue;
+      const auto now = Clock::now();
+      for (auto& r : s.batch) {
+        finish_request(*r, s.hbuf);
+        r->t_done = now;
+        r->done = true;
+        S->completed++;
+      }
+      S->mem_in_use -= s.bytes;
+      s.batch.clear();
+      s.busy = false;
+      progressed = true;
+      S->cv.notify_all();
+    }
+    // 2. admissions: fill every free slot with pending requests (FIFO)
+    for (auto& s : S->slots) {
+      if (s.busy || S->pending.empty()) continue;
+      const size_t budget = (size_t)S->cfg.mem_budget_bytes;
+      std::vector<std::shared_ptr<Request>> b;
+      int64_t paths = 0;
+      size_t bytes = 0;
+      while (!S->pending.empty() && (int)b.size() < max_sys) {
+        auto& r = S->pending.front();
+        const size_t need = r->dev_bytes;
+        if (!b.empty() && (paths + r->npaths > max_paths)) break;
+        if (S->mem_in_use + bytes + need > budget) break;
+        bytes += need;
+        paths += r->npaths;
+        b.push_back(r);
+        S->pending.pop_front();
+      }
+      if (b.empty()) break;  // memory budget exhausted: wait for completions
+      s.batch = b;
+      int st = launch_batch(S, s);
+      if (st != PHC_OK) {
+        for (auto& r : s.batch) {
+          r->status = st;
+          r->t_done = Clock::now();
+          r->done = true;
+          S->completed++;
+        }
+        s.batch.clear();
+        S->cv.notify_all();
+        continue;
+      }
+      s.busy = true;
+      S->mem_in_use += s.bytes;
+      S->batches++;
+      progressed = true;
+    }
+    bool any_busy = false;
+    for (auto& s : S->slots) any_busy |= s.busy;
+    if (S->stop && !any_busy) break;
+    if (!progressed) {
+      if (any_busy)
+        S->cv.wait_for(lk, std::chrono::microseconds(50));
+      else
+        S->cv.wait_for(lk, std::chrono::milliseconds(20));
+    }
+  }
+  // abort what never started
+  for (auto& r : S->pending) {
+    r->status = PHC_ERR_ABORTED;
+    r->done = true;
+  }
+  S->pending.clear();
+  S->cv.notify_all();
+}
+
+}  // namespace
+}  // namespace phc
+
+extern "C" {
+
+int32_t phc_server_create(const phc_server_config* cfg, phc_server** out) {
+  if (!cfg || !out) return PHC_ERR_INVALID_INPUT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1 || cfg->device < 0 ||
+      cfg->device >= count) {
+    set_last_error("no CUDA device for the server");
+    return PHC_ERR_NO_DEVICE;
+  }
+  std::unique_ptr<phc_server> S(new (std::nothrow) phc_server());
+  if (!S) return PHC_ERR_OOM;
+  S->cfg = *cfg;
+  if (S->cfg.nslots < 1) S->cfg.nslots = 4;
+  if (S->cfg.mem_budget_bytes <= 0) S->cfg.mem_budget_bytes = (int64_t)1 << 30;
+  S->cfg.gpu.device = cfg->device;
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  S->slots.resize(S->cfg.nslots);
+  for (auto& s : S->slots) {
+    e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "server stream");
+    e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, "server event");
+  }
+  phc_server* raw = S.release();
+  raw->engine = std::thread(engine_main, raw);
+  *out = raw;
+  return PHC_OK;
+}
+
+int32_t phc_server_submit(phc_server* S, const phc_system* sys, const phc_solve_options* opts,
+                          uint64_t* ticket) {
+  if (!S || !ticket) return PHC_ERR_BAD_HANDLE;
+  const phc_solve_options so = opts ? *opts : solve_defaults();
+  int st = validate_options(&so);
+  if (st != PHC_OK) return st;
+  st = validate_system(sys);
+  if (st != PHC_OK) return st;
+  auto r = std::make_shared<Request>();
+  r->n = sys->n;
+  r->first.assign(sys->first, sys->first + sys->n + 1);
+  r->deg.assign(sys->deg, sys->deg + sys->n);
+  r->hexps.assign(sys->hexps, sys->hexps + (size_t)sys->nterms * (sys->n + 1));
+  r->coefs.assign(sys->coefs, sys->coefs + 2 * (size_t)sys->nterms);
+  r->opts = so;
+  st = homotopy_init(sys, so.seed, &r->hom);  // gen%seed + hom%init
+  if (st != PHC_OK) return st;
+  const phc_system v = r->view();
+  const phc_homotopy hv = r->hom.view();
+  st = build_plan(&v, &hv, &r->plan);
+  if (st != PHC_OK) return st;
+  r->npaths = r->hom.nstart;
+  st = resolve_launch(r->plan, S->cfg.gpu, S->cfg.device, &r->cfg);
+  if (st != PHC_OK) return st;
+  r->dev_bytes = up256(r->plan.bytes.size()) + up256((size_t)r->npaths * sizeof(phc_path_out)) +
+                 up256((size_t)r->npaths * (r->n + 1) * 16) + up256((size_t)r->npaths * r->n * 16);
+  if (r->dev_bytes > (size_t)S->cfg.mem_budget_bytes) {
+    set_last_error("request larger than the server's memory budget");
+    return PHC_ERR_ADMISSION;
+  }
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) return PHC_ERR_ABORTED;
+    r->ticket = S->next_ticket++;
+    S->all[r->ticket] = r;
+    S->pending.push_back(r);
+    S->submitted++;
+  }
+  S->cv.notify_all();
+  *ticket = r->ticket;
+  return PHC_OK;
+}
+
+int32_t phc_server_poll(phc_server* S, uint64_t ticket, int32_t* done) {
+  if (!S || !done) return PHC_ERR_BAD_HANDLE;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->all.find(ticket);
+  if (it == S->all.end()) return PHC_ERR_BAD_HANDLE;
+  *done = it->second->done ? 1 : 0;
+  return PHC_OK;
+}
+
+int32_t phc_server_wait(phc_server* S, uint64_t ticket, int64_t timeout_ms) {
+  if (!S) return PHC_ERR_BAD_HANDLE;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->all.find(ticket);
+  if (it == S->all.end()) return PHC_ERR_BAD_HANDLE;
+  auto r = it->second;
+  auto pred = [&] { return r->done; };
+  if (timeout_ms < 0) {
+    S->cv.wait(lk, pred);
+  } else if (!S->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred)) {
+    return PHC_ERR_NOT_READY;
+  }
+  return PHC_OK;
+}
+
+int64_t phc_server_npaths(phc_server* S, uint64_t ticket) {
+  if (!S) return 0;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->all.find(ticket);
+  return it == S->all.end() ? 0 : it->second->npaths;
+}
+
+int32_t phc_server_result(phc_server* S, uint64_t ticket, phc_solve_result* res,
+                          double* latency_s) {
+  if (!S || !res) return PHC_ERR_BAD_HANDLE;
+  std::shared_ptr<Request> r;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->all.find(ticket);
+    if (it == S->all.end()) return PHC_ERR_BAD_HANDLE;
+    r = it->second;
+    if (!r->done) return PHC_ERR_NOT_READY;
+    S->all.erase(it);
+  }
+  if (latency_s)
+    *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+  if (r->status != PHC_OK) return r->status;
+  const int n = r->n;
+  res->counts = r->counts;
+  if (res->paths) std::memcpy(res->paths, r->paths.data(), r->paths.size() * sizeof(phc_path_out));
+  if (res->z) std::memcpy(res->z, r->z.data(), r->z.size() * sizeof(double));
+  if (res->x) std::memcpy(res->x, r->x.data(), r->x.size() * sizeof(double));
+  if (res->solutions)
+    std::memcpy(res->solutions, r->sols.data(), (size_t)r->counts.nsolutions * n * 2 * sizeof(double));
+  if (res->real_solutions)
+    std::memcpy(res->real_solutions, r->realsols.data(), (size_t)r->counts.nreal * n * sizeof(double));
+  if (res->singular_solutions)
+    std::memcpy(res->singular_solutions, r->ssols.data(),
+                (size_t)r->counts.nsingular * n * 2 * sizeof(double));
+  if (res->multiplicities)
+    std::memcpy(res->multiplicities, r->mult.data(), (size_t)r->counts.nsingular * sizeof(int32_t));
+  return PHC_OK;
+}
+
+int32_t phc_server_stats(phc_server* S, int64_t* submitted, int64_t* completed, int64_t* batches,
+                         int64_t* in_flight) {
+  if (!S) return PHC_ERR_BAD_HANDLE;
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (submitted) *submitted = S->submitted;
+  if (completed) *completed = S->completed;
+  if (batches) *batches = S->batches;
+  if (in_flight) {
+    int64_t k = 0;
+    for (auto& s : S->slots) k += s.busy ? (int64_t)s.batch.size() : 0;
+    *in_flight = k;
+  }
+  return PHC_OK;
+}
+
+int32_t phc_server_destroy(phc_server* S) {
+  if (!S) return PHC_ERR_BAD_HANDLE;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->cv.notify_all();
+  if (S->engine.joinable()) S->engine.join();
+  cudaSetDevice(S->cfg.device);
+  for (auto& s : S->slots) {
+    if (s.stream) cudaStreamSynchronize(s.stream);
+    if (s.dbuf) cudaFree(s.dbuf);
+    if (s.hbuf) cudaFreeHost(s.hbuf);
+    if (s.counters) cudaFree(s.counters);
+    if (s.done) cudaEventDestroy(s.done);
+    if (s.stream) cudaStreamDestroy(s.stream);
+  }
+  delete S;
+  return PHC_OK;
+}
+
+}  // extern "C"

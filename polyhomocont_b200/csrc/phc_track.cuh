@@ -1,0 +1,905 @@
+// phc_track.cuh -- the path-tracking kernel: one warp tracks one path
+// through start_solution, the predictor-corrector tracker, the Cauchy end
+// game and the classification numerics (src/solve.f90:190-198, :217-328).
+//
+// The reference's nested procedures (track_segment inside loops inside
+// cauchy_endgame inside endpoint) are flattened into one warp-uniform
+// state machine whose every step either changes control state or runs
+// exactly one "unit": an evaluation of H(z,t) (and H_z, H_t), optionally
+// followed by the LU factorization and one or N solves. There is a single
+// call site of the unit per precision, so the large unrolled LU/solve code
+// exists once per precision in the kernel binary, and the same machine
+// serves the predictor, the corrector, the end game's backward errors,
+// refine and cond1.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "phc_device.cuh"
+#include "phc_internal.h"
+
+namespace phc {
+
+enum UnitKind : int { UK_TANGENT = 0, UK_NEWTON = 1, UK_BACKERR = 2, UK_COND = 3,
+                      UK_REFINE = 4 };
+
+struct UnitRes {
+  cd x;       // solution component of this lane
+  cd h;       // residual component of this lane (UK_COND)
+  double a1;  // UK_BACKERR: ||h||_inf; UK_COND: cond1
+  double a2;  // UK_BACKERR: max row sum of |H_z|
+  bool ok;    // LU nonsingular
+};
+
+// One unit in precision T (row/LU type). f64res selects FP64 evaluation of
+// F^h for the residual (always true when T is double).
+template <int NM, typename T>
+__device__ __forceinline__ void run_unit(const PlanHeader& P, const Rec* recs,
+                                         const WarpWS& ws, int kind, bool f64res, cd zin,
+                                         cd t, cd dt, int lane, UnitRes& u) {
+  cpx<T> a[NM];
+  cd h, ht;
+  evaluate<NM, T>(P, recs, ws, zin, t, lane, f64res || sizeof(T) == 8, a, h, ht);
+  const int N = P.N;
+  if (kind == UK_BACKERR) {
+    // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
+    // absolute row sum of H_z
+    double rs = 0.0;
+#pragma unroll
+    for (int j = 0; j < NM; ++j)
+      if (j < N) rs += (double)cabs(a[j]);
+    u.a1 = warp_max_nonneg(lane < N ? cabs(h) : 0.0);
+    u.a2 = warp_max_nonneg(lane < N ? rs : 0.0);
+    u.ok = true;
+    return;
+  }
+  double anorm = 0.0;
+  if (kind == UK_COND) {
+    // cond1, src/linalg.f90:135-174: ||A||_1 = largest column sum
+    u.h = h;
+#pragma unroll
+    for (int j = 0; j < NM; ++j) {
+      if (j < N) {
+        double c = warp_sum(lane < N ? (double)cabs(a[j]) : 0.0);
+        anorm = fmax(anorm, c);
+      }
+    }
+  }
+  int pstep;
+  unsigned piv[(NM + 3) / 4];
+  u.ok = lu_rows<NM, T>(a, N, lane, pstep, piv, reinterpret_cast<cpx<T>*>(ws.prow));
+  if (!u.ok) {
+    u.a1 = DBL_MAX;  // cond1 of an exactly singular matrix
+    return;
+  }
+  const int nsolve = (kind == UK_COND) ? N : 1;
+  const cd rhs0 = (kind == UK_TANGENT) ? -(ht * dt) : -h;
+  double ainv = 0.0;
+  for (int jj = 0; jj < nsolve; ++jj) {
+    cpx<T> rhs;
+    if (kind == UK_COND)
+      rhs = (lane == jj) ? cone<T>() : czero<T>();
+    else
+      rhs = ccast<T>(rhs0);
+    const cpx<T> x = solve_rows<NM, T>(a, N, lane, pstep, piv, rhs);
+    if (kind == UK_COND) {
+      double s = warp_sum(lane < N ? (double)cabs(x) : 0.0);
+      ainv = fmax(ainv, s);
+    } else {
+      u.x = ccast<double>(x);
+    }
+  }
+  if (kind == UK_COND) u.a1 = anorm * ainv;
+}
+
+enum Pc : int {
+  PC_START,
+  PC_SEG_BEGIN,
+  PC_SEG_ATTEMPT,
+  PC_SEG_AFTER_UNIT,
+  PC_SEG_END,
+  PC_MAIN_DONE,
+  PC_EG_INIT,
+  PC_EG_TOP,
+  PC_EG_AFTER_LOOPS,
+  PC_EG_AFTER_RECORD_MAIN,
+  PC_EG_RADIAL,
+  PC_EG_AFTER_RADIAL,
+  PC_EG_AFTER_FALLBACK,
+  PC_LOOPS_BEGIN,
+  PC_LOOP_ARC,
+  PC_LOOP_AFTER_ARC,
+  PC_RECORD,
+  PC_RECORD_AFTER,
+  PC_EG_DONE,
+  PC_CL_START,
+  PC_CL_AFTER_COND1,
+  PC_CL_AFTER_REFINE,
+  PC_CL_COND2,
+  PC_CL_AFTER_COND2,
+  PC_CL_FINAL,
+  PC_FINISH,
+};
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kEps = DBL_EPSILON;
+constexpr double kTiny = DBL_MIN;
+constexpr double kHuge = DBL_MAX;
+
+__device__ __forceinline__ double vnorm(cd v, int lane, int N) {
+  return warp_max_nonneg(lane < N ? cabs(v) : 0.0);
+}
+
+// better(), src/endgame.f90:287-311
+__device__ __forceinline__ bool better(double resid, double err, double best_resid,
+                                       double best_err, double residual_tol) {
+  const bool valid = resid <= residual_tol;
+  const bool best_valid = best_resid <= residual_tol;
+  if (valid != best_valid) return valid;
+  return err < best_err;
+}
+
+// Segment t(s) and dt/ds of the segment stored in the warp state.
+__device__ __forceinline__ cd seg_t(const WarpState& st, double s) {  // :142-162
+  if (!st.seg_arc) {
+    const cd t0 = mkc<double>(st.seg_t0[0], st.seg_t0[1]);
+    const cd t1 = mkc<double>(st.seg_t1[0], st.seg_t1[1]);
+    if (s >= 1.0) return t1;
+    return t0 + s * (t1 - t0);
+  }
+  double sn, cs;
+  sincos(st.seg_th0 + s * st.seg_dth, &sn, &cs);
+  return st.seg_r * mkc<double>(cs, sn);
+}
+__device__ __forceinline__ cd seg_dt(const WarpState& st, double s) {  // :164-177
+  if (!st.seg_arc)
+    return mkc<double>(st.seg_t1[0] - st.seg_t0[0], st.seg_t1[1] - st.seg_t0[1]);
+  return mkc<double>(0.0, st.seg_dth) * seg_t(st, s);
+}
+
+#define LV(f) (reinterpret_cast<cd*>(st.f)[lane])
+#define LDV(f) lds(&LV(f))
+#define STV(f, v) sts(&LV(f), (v))
+
+// Tracks path k (1-based) and writes its record, z and x.
+template <int NM, int PREC>
+__device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, const WarpWS& ws,
+                          WarpState& st, const KOpts& O, int64_t k, int lane,
+                          phc_path_out* rec, double* zo, double* xo) {
+  const phc_tracker_options& TO = O.so.tracker;
+  const phc_endgame_options& EO = O.so.endgame;
+  const int n = P.n, N = P.N;
+  constexpr bool kMixed = (PREC == PHC_PREC_MIXED);
+
+  // hot lane vectors (component j in lane j)
+  cd z = czero<double>(), zs = z, zp = z, ksum = z, zin = z;
+  // hot uniform state of the segment being tracked
+  double s = 0.0, step = 0.0, ds = 0.0, sn = 0.0, dnorm_prev = kHuge;
+  int nsucc = 0, sacc = 0, srej = 0, sstat = PHC_PATH_SUCCESS, stage = 0;
+  bool att64 = true;
+  // pending unit
+  int uk = UK_TANGENT, pc_after = PC_FINISH;
+  bool u_f32 = false, u_f64res = true;
+  cd tin = z, dtin = z;
+  UnitRes U;
+  U.x = U.h = czero<double>();
+  U.a1 = U.a2 = 0.0;
+  U.ok = true;
+
+  // path result defaults (type(path_result), src/solve.f90:86-119)
+  st.p_status = PHC_PATH_SUCCESS;
+  st.p_wind = st.p_egs = st.p_nacc = st.p_nrej = 0;
+  st.p_t = 1.0;
+  st.p_ege = st.p_cond = st.p_resid = 0.0;
+  st.p_atinf = st.p_sing = st.p_real = 0;
+  st.c_tan = st.c_new = st.c_ref = st.c_eval = st.c_cond = st.c_retry = 0;
+  st.units = 0;
+  st.sticky = 0;
+  STV(xv, czero<double>());
+
+  int pc = PC_START;
+  for (;;) {
+    bool want = false;
+    while (!want) {
+      switch (pc) {
+        case PC_START: {
+          // tdh_start_solution, src/homotopy.f90:151-177
+          if (lane < n) {
+            const int d = P.deg[lane];
+            const int64_t digit = ((k - 1) / P.radix[lane]) % d;
+            const double phi = (P.argb[lane] + 2.0 * kPi * (double)digit) / (double)d;
+            double sp, cp;
+            sincos(phi, &sp, &cp);
+            z = mkc<double>(cp, sp);
+          } else if (lane == n) {
+            z = cone<double>();
+          }
+          const cd pz = (lane < N) ? mkc<double>(P.patch[lane][0], P.patch[lane][1]) * z
+                                   : czero<double>();
+          const cd sum = warp_csum(pz);
+          if (lane < N) z = cdiv(z, sum);
+          // track_path(hom, z, 1, t_end), src/solve.f90:230-232
+          st.seg_arc = 0;
+          st.seg_t0[0] = 1.0;
+          st.seg_t0[1] = 0.0;
+          st.seg_t1[0] = O.so.use_endgame ? EO.t_start : 0.0;
+          st.seg_t1[1] = 0.0;
+          st.o_step_init = TO.step_init;
+          st.o_step_max = TO.step_max;
+          st.o_grow = TO.grow_after;
+          zs = z;
+          st.seg_cont = PC_MAIN_DONE;
+          pc = PC_SEG_BEGIN;
+          break;
+        }
+
+        // ---------------- track_segment, src/tracker.f90:196-264 -------------
+        case PC_SEG_BEGIN:
+          s = 0.0;
+          step = fmin(st.o_step_init, st.o_step_max);
+          nsucc = 0;
+          sacc = 0;
+          srej = 0;
+          sstat = PHC_PATH_SUCCESS;
+          pc = PC_SEG_ATTEMPT;
+          break;
+
+        case PC_SEG_ATTEMPT: {
+          if (!(s < 1.0)) {
+            pc = PC_SEG_END;
+            break;
+          }
+          if (sacc + srej >= TO.max_steps || st.units > O.max_units) {
+            sstat = PHC_PATH_FAILED_MAX_STEPS;
+            pc = PC_SEG_END;
+            break;
+          }
+          ds = fmin(step, 1.0 - s);
+          sn = s + ds;
+          if (1.0 - sn <= 1.0e-3 * step) {
+            sn = 1.0;
+            ds = 1.0 - s;
+          }
+          const int sticky = st.sticky;
+          att64 = !kMixed || sticky > 0;
+          if (sticky > 0) st.sticky = sticky - 1;
+          // predict_rk4 stage 1: tangent at (z, s), src/tracker.f90:283
+          stage = 0;
+          uk = UK_TANGENT;
+          u_f32 = !att64;
+          u_f64res = att64;
+          zin = zs;
+          tin = seg_t(st, s);
+          dtin = seg_dt(st, s);
+          pc_after = PC_SEG_AFTER_UNIT;
+          want = true;
+          break;
+        }
+
+        case PC_SEG_AFTER_UNIT: {
+          int outcome = 0;  // 1 accept, 2 reject
+          if (stage < 4) {
+            ++st.c_tan;
+            if (!U.ok) {
+              outcome = 2;
+            } else {
+              // predict_rk4, src/tracker.f90:266-293
+              const cd kk = U.x;
+              double s_in = s;
+              if (stage == 0) {
+                ksum = kk;
+                zin = zs + (0.5 * ds) * kk;
+                s_in = s + 0.5 * ds;
+              } else if (stage == 1) {
+                ksum = ksum + 2.0 * kk;
+                zin = zs + (0.5 * ds) * kk;
+                s_in = s + 0.5 * ds;
+              } else if (stage == 2) {
+                ksum = ksum + 2.0 * kk;
+                zin = zs + ds * kk;
+                s_in = s + ds;
+              } else {
+                ksum = ksum + kk;
+                zp = zs + (ds / 6.0) * ksum;
+              }
+              if (stage < 3) {
+                ++stage;
+                uk = UK_TANGENT;
+                tin = seg_t(st, s_in);
+                dtin = seg_dt(st, s_in);
+              } else {
+                // newton_correct at t(sn), src/tracker.f90:319-360
+                stage = 4;
+                dnorm_prev = kHuge;
+                uk = UK_NEWTON;
+                u_f64res = true;
+                zin = zp;
+                tin = seg_t(st, sn);
+              }
+              pc_after = PC_SEG_AFTER_UNIT;
+              want = true;
+              break;
+            }
+          } else {
+            ++st.c_new;
+            const int it = stage - 3;
+            if (!U.ok) {
+              outcome = 2;
+            } else {
+              zp = zp + U.x;
+              const double dnorm = vnorm(U.x, lane, N);
+              const double znorm = vnorm(zp, lane, N);
+              if (dnorm <= TO.corrector_tol * znorm) {
+                outcome = 1;
+              } else if (it > 1 && dnorm > TO.contraction * dnorm_prev) {
+                outcome = 2;
+              } else {
+                dnorm_prev = dnorm;
+                if (it >= TO.corrector_maxit) {
+                  outcome = 2;
+                } else {
+                  ++stage;
+                  uk = UK_NEWTON;
+                  zin = zp;
+                  pc_after = PC_SEG_AFTER_UNIT;
+                  want = true;
+                  break;
+                }
+              }
+            }
+          }
+          if (outcome == 1) {
+            zs = zp;
+            s = sn;
+            ++sacc;
+            ++nsucc;
+            if (nsucc >= st.o_grow) {
+              step = fmin(2.0 * step, st.o_step_max);
+              nsucc = 0;
+            }
+            pc = PC_SEG_ATTEMPT;
+          } else {
+            if (kMixed && !att64) {
+              // the FP32 attempt failed: redo the same step in FP64 before
+              // counting a rejection, and stay in FP64 for a few steps
+              att64 = true;
+              st.sticky = O.fp64_sticky;
+              ++st.c_retry;
+              stage = 0;
+              uk = UK_TANGENT;
+              u_f32 = false;
+              u_f64res = true;
+              zin = zs;
+              tin = seg_t(st, s);
+              dtin = seg_dt(st, s);
+              pc_after = PC_SEG_AFTER_UNIT;
+              want = true;
+              break;
+            }
+            ++srej;
+            nsucc = 0;
+            step = 0.5 * step;
+            if (step < TO.step_min) {
+              sstat = PHC_PATH_FAILED_MIN_STEP;
+              pc = PC_SEG_END;
+            } else {
+              pc = PC_SEG_ATTEMPT;
+            }
+          }
+          break;
+        }
+
+        case PC_SEG_END:
+          pc = st.seg_cont;
+          break;
+
+        // ---------------- endpoint, src/solve.f90:217-252 ----------------------
+        case PC_MAIN_DONE:
+          z = zs;
+          st.p_status = sstat;
+          st.p_t = seg_t(st, s).re;
+          st.p_nacc = sacc;
+          st.p_nrej = srej;
+          if (sstat != PHC_PATH_SUCCESS)
+            pc = PC_FINISH;
+          else if (!O.so.use_endgame)
+            pc = PC_CL_START;
+          else
+            pc = PC_EG_INIT;
+          break;
+
+        // ---------------- cauchy_endgame, src/endgame.f90:124-267 --------------
+        case PC_EG_INIT:
+          st.eg_segstep = 1.0;  // segopts: step_init = step_max = 1, grow_after = 2
+          st.eg_status = PHC_ENDGAME_FAILED;
+          STV(resz, z);
+          st.r = EO.t_start;
+          st.have_prev = 0;
+          st.best_resid = kHuge;
+          st.gate = 0;
+          st.dprev = -1.0;
+          st.cest = -1.0;
+          st.cest_prev = -1.0;
+          st.max_loops = EO.max_winding;
+          st.eg_wind = 0;
+          st.eg_error = kHuge;
+          st.eg_residual = kHuge;
+          st.eg_radius = 0.0;
+          st.eg_nacc = 0;
+          st.eg_nrej = 0;
+          pc = PC_EG_TOP;
+          break;
+
+        case PC_EG_TOP:
+          if (st.gate || st.r < EO.loop_radius) {
+            if (!st.gate) st.max_loops = EO.max_winding;
+            st.lp_max = st.max_loops;
+            st.lp_cont = PC_EG_AFTER_LOOPS;
+            pc = PC_LOOPS_BEGIN;
+          } else {
+            st.lp_ok = 0;
+            pc = PC_EG_AFTER_LOOPS;
+          }
+          break;
+
+        case PC_EG_AFTER_LOOPS:
+          if (!st.lp_ok) {
+            st.have_prev = 0;
+            st.gate = 0;
+            pc = PC_EG_RADIAL;
+          } else {
+            st.rec_cont = PC_EG_AFTER_RECORD_MAIN;
+            pc = PC_RECORD;
+          }
+          break;
+
+        case PC_EG_AFTER_RECORD_MAIN:
+          if (st.eg_status == PHC_ENDGAME_CONVERGED) {
+            pc = PC_EG_DONE;
+          } else {
+            STV(prev, LDV(est));
+            st.have_prev = 1;
+            pc = PC_EG_RADIAL;
+          }
+          break;
+
+        case PC_EG_RADIAL: {
+          const double rnew = EO.radius_factor * st.r;
+          st.rnew = rnew;
+          if (rnew < EO.radius_min) {
+            pc = PC_EG_DONE;
+            break;
+          }
+          STV(zold, z);
+          zs = z;
+          st.seg_arc = 0;
+          st.seg_t0[0] = st.r;
+          st.seg_t0[1] = 0.0;
+          st.seg_t1[0] = rnew;
+          st.seg_t1[1] = 0.0;
+          st.o_step_init = st.eg_segstep;
+          st.o_step_max = 1.0;
+          st.o_grow = 2;
+          st.seg_cont = PC_EG_AFTER_RADIAL;
+          pc = PC_SEG_BEGIN;
+          break;
+        }
+
+        case PC_EG_AFTER_RADIAL: {
+          z = zs;
+          st.eg_segstep = fmin(fmax(step, TO.step_min), 1.0);
+          st.eg_nacc += sacc;
+          st.eg_nrej += srej;
+          const cd zold = LDV(zold);
+          if (sstat != PHC_PATH_SUCCESS) {
+            z = zold;
+            if (!(st.gate || st.r < EO.loop_radius)) {
+              st.lp_max = EO.max_winding;
+              st.lp_cont = PC_EG_AFTER_FALLBACK;
+              pc = PC_LOOPS_BEGIN;
+            } else {
+              pc = PC_EG_DONE;
+            }
+            break;
+          }
+          st.r = st.rnew;
+          // winding number estimate from the radial differences
+          const double d = vnorm(z - zold, lane, N);
+          const double dprev = st.dprev;
+          if (!st.gate && dprev > 0.0 && d > 0.0) {
+            const double cest_prev = st.cest;
+            double cest = -1.0;
+            if (dprev > d) cest = log(1.0 / EO.radius_factor) / log(dprev / d);
+            st.cest_prev = cest_prev;
+            st.cest = cest;
+            if (cest >= 0.5 && cest <= (double)EO.max_winding + 0.5 && cest_prev > 0.0) {
+              if (fabs(cest - cest_prev) <= EO.winding_agreement * fmax(1.0, cest)) {
+                st.gate = 1;
+                st.max_loops = min(EO.max_winding, 2 * (int)llround(cest) + 2);
+              }
+            }
+          }
+          st.dprev = d;
+          pc = PC_EG_TOP;
+          break;
+        }
+
+        case PC_EG_AFTER_FALLBACK:
+          st.have_prev = 0;
+          if (st.lp_ok) {
+            st.rec_cont = PC_EG_DONE;
+            pc = PC_RECORD;
+          } else {
+            pc = PC_EG_DONE;
+          }
+          break;
+
+        case PC_LOOPS_BEGIN:
+          st.lp_dth = 2.0 * kPi / (double)EO.nsamples;
+          st.lp_floor = 10.0 * TO.corrector_tol * vnorm(z, lane, N);
+          zs = z;
+          STV(zsum, czero<double>());
+          st.lp_nsamp = 0;
+          st.lp_spacing = kHuge;
+          st.lp_c = 1;
+          st.lp_j = 1;
+          pc = PC_LOOP_ARC;
+          break;
+
+        case PC_LOOP_ARC:
+          STV(zsum, LDV(zsum) + zs);
+          ++st.lp_nsamp;
+          STV(zprev, zs);
+          st.seg_arc = 1;
+          st.seg_r = st.r;
+          st.seg_th0 = (double)(st.lp_j - 1) * st.lp_dth;
+          st.seg_dth = st.lp_dth;
+          st.o_step_init = st.eg_segstep;
+          st.o_step_max = 1.0;
+          st.o_grow = 2;
+          st.seg_cont = PC_LOOP_AFTER_ARC;
+          pc = PC_SEG_BEGIN;
+          break;
+
+        case PC_LOOP_AFTER_ARC: {
+          st.eg_segstep = fmin(fmax(step, TO.step_min), 1.0);
+          st.eg_nacc += sacc;
+          st.eg_nrej += srej;
+          if (sstat != PHC_PATH_SUCCESS) {
+            st.lp_ok = 0;
+            pc = st.lp_cont;
+            break;
+          }
+          st.lp_spacing = fmin(st.lp_spacing, vnorm(zs - LDV(zprev), lane, N));
+          const int j = st.lp_j + 1;
+          st.lp_j = j;
+          if (j <= EO.nsamples) {
+            pc = PC_LOOP_ARC;
+            break;
+          }
+          if (vnorm(zs - z, lane, N) <= fmax(EO.closure_factor * st.lp_spacing, st.lp_floor)) {
+            const double inv = (double)st.lp_nsamp;
+            const cd zsum = LDV(zsum);
+            STV(est, mkc<double>(zsum.re / inv, zsum.im / inv));
+            st.cw = st.lp_c;
+            st.lp_ok = 1;
+            pc = st.lp_cont;
+            break;
+          }
+          const int c = st.lp_c + 1;
+          st.lp_c = c;
+          st.lp_j = 1;
+          if (c <= st.lp_max) {
+            pc = PC_LOOP_ARC;
+          } else {
+            st.lp_ok = 0;
+            pc = st.lp_cont;
+          }
+          break;
+        }
+
+        case PC_RECORD: {  // record(), src/endgame.f90:240-265
+          const cd est = LDV(est);
+          double err = kHuge;
+          if (st.have_prev)
+            err = vnorm(est - LDV(prev), lane, N) / fmax(vnorm(est, lane, N), kTiny);
+          st.rec_err = err;
+          uk = UK_BACKERR;
+          u_f32 = false;
+          u_f64res = true;
+          zin = est;
+          tin = czero<double>();
+          dtin = czero<double>();
+          pc_after = PC_RECORD_AFTER;
+          want = true;
+          break;
+        }
+
+        case PC_RECORD_AFTER: {
+          ++st.c_eval;
+          const double err = st.rec_err;
+          const double resid = U.a1 / fmax(U.a2 * vnorm(zin, lane, N), kTiny);
+          if (st.eg_status == PHC_ENDGAME_FAILED ||
+              better(resid, err, st.best_resid, st.eg_error, EO.residual_tol)) {
+            st.eg_status = PHC_ENDGAME_NOT_CONVERGED;
+            STV(resz, zin);
+            st.eg_wind = st.cw;
+            st.eg_error = err;
+            st.eg_residual = resid;
+            st.eg_radius = st.r;
+            st.best_resid = resid;
+          }
+          if (err <= EO.tol && resid <= EO.residual_tol) st.eg_status = PHC_ENDGAME_CONVERGED;
+          pc = st.rec_cont;
+          break;
+        }
+
+        case PC_EG_DONE:
+          st.p_nacc += st.eg_nacc;
+          st.p_nrej += st.eg_nrej;
+          if (st.eg_status == PHC_ENDGAME_FAILED) {
+            st.p_status = PHC_PATH_ENDGAME_FAILED;
+            pc = PC_FINISH;
+          } else {
+            z = LDV(resz);
+            st.p_t = 0.0;
+            st.p_wind = st.eg_wind;
+            st.p_egs = st.eg_status;
+            st.p_ege = st.eg_error;
+            pc = PC_CL_START;
+          }
+          break;
+
+        // ---------------- classify, src/solve.f90:288-328 ---------------------
+        case PC_CL_START:
+          uk = UK_COND;
+          u_f32 = false;
+          u_f64res = true;
+          zin = z;
+          tin = czero<double>();
+          dtin = czero<double>();
+          pc_after = PC_CL_AFTER_COND1;
+          want = true;
+          break;
+
+        case PC_CL_AFTER_COND1: {
+          ++st.c_eval;
+          ++st.c_cond;
+          st.p_cond = U.a1;
+          STV(hsave, U.h);
+          const bool sing = st.p_wind > 1 || U.a1 > O.so.singular_cond;
+          st.p_sing = sing ? 1 : 0;
+          if (!sing && O.so.refine_maxit >= 1) {
+            // refine, src/solve.f90:254-286
+            st.rf_it = 1;
+            dnorm_prev = kHuge;
+            uk = UK_REFINE;
+            zin = z;
+            pc_after = PC_CL_AFTER_REFINE;
+            want = true;
+          } else {
+            pc = sing ? PC_CL_FINAL : PC_CL_COND2;
+          }
+          break;
+        }
+
+        case PC_CL_AFTER_REFINE: {
+          ++st.c_ref;
+          if (!U.ok) {
+            pc = PC_CL_COND2;
+            break;
+          }
+          const double dnorm = vnorm(U.x, lane, N);
+          if (dnorm > dnorm_prev) {
+            pc = PC_CL_COND2;
+            break;
+          }
+          z = z + U.x;
+          if (dnorm <= 4.0 * kEps * vnorm(z, lane, N)) {
+            pc = PC_CL_COND2;
+            break;
+          }
+          dnorm_prev = dnorm;
+          const int it = st.rf_it + 1;
+          st.rf_it = it;
+          if (it > O.so.refine_maxit) {
+            pc = PC_CL_COND2;
+            break;
+          }
+          uk = UK_REFINE;
+          zin = z;
+          pc_after = PC_CL_AFTER_REFINE;
+          want = true;
+          break;
+        }
+
+        case PC_CL_COND2:
+          uk = UK_COND;
+          zin = z;
+          pc_after = PC_CL_AFTER_COND2;
+          want = true;
+          break;
+
+        case PC_CL_AFTER_COND2:
+          ++st.c_eval;
+          ++st.c_cond;
+          st.p_cond = U.a1;
+          STV(hsave, U.h);
+          pc = PC_CL_FINAL;
+          break;
+
+        case PC_CL_FINAL: {
+          const double znorm = vnorm(z, lane, N);
+          const double ri =
+              (lane < n) ? cabs(LDV(hsave)) / rpowi(znorm, P.deg[lane]) : 0.0;
+          st.p_resid = warp_max_nonneg(ri);
+          const cd w = shfl(z, n);
+          const bool atinf =
+              cabs(w) <= fmax(O.so.infinity_tol, 10.0 * fmin(st.p_ege, 1.0e-4)) * znorm;
+          st.p_atinf = atinf ? 1 : 0;
+          if (!atinf) {
+            // x = z(1:n)/w, src/solve.f90:322-326
+            const cd xv = (lane < n) ? cdiv(z, w) : czero<double>();
+            STV(xv, xv);
+            const double imax = warp_max_nonneg(lane < n ? fabs(xv.im) : 0.0);
+            const double xnorm = vnorm(xv, lane, n);
+            st.p_real = (imax <= O.so.real_tol * fmax(1.0, xnorm)) ? 1 : 0;
+          }
+          pc = PC_FINISH;
+          break;
+        }
+
+        case PC_FINISH: {
+          __syncwarp();
+          if (lane == 0) {
+            phc_path_out o;
+            o.status = st.p_status;
+            o.winding_number = st.p_wind;
+            o.endgame_status = st.p_egs;
+            o.at_infinity = st.p_atinf;
+            o.singular = st.p_sing;
+            o.is_real = st.p_real;
+            o.naccepted = st.p_nacc;
+            o.nrejected = st.p_nrej;
+            o.solution_index = 0;
+            o.singular_index = 0;
+            o.n_tangent = st.c_tan;
+            o.n_newton = st.c_new;
+            o.n_refine = st.c_ref;
+            o.n_eval = st.c_eval;
+            o.n_cond = st.c_cond;
+            o.n_fp64_retry = st.c_retry;
+            o.t = st.p_t;
+            o.endgame_error = st.p_ege;
+            o.cond = st.p_cond;
+            o.residual = st.p_resid;
+            *rec = o;
+          }
+          if (lane < N) {
+            zo[2 * lane] = z.re;
+            zo[2 * lane + 1] = z.im;
+          }
+          if (xo != nullptr && lane < n) {
+            const cd xv = LDV(xv);
+            xo[2 * lane] = xv.re;
+            xo[2 * lane + 1] = xv.im;
+          }
+          __syncwarp();
+          return;
+        }
+      }
+    }
+    // ---- run the requested unit ----
+    if (kMixed && u_f32)
+      run_unit<NM, float>(P, recs, ws, uk, u_f64res, zin, tin, dtin, lane, U);
+    else
+      run_unit<NM, double>(P, recs, ws, uk, true, zin, tin, dtin, lane, U);
+    ++st.units;
+    pc = pc_after;
+  }
+}
+
+#undef LV
+#undef LDV
+#undef STV
+
+template <int NM, int PREC>
+__global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int tid = threadIdx.x;
+  {
+    const int4* src = reinterpret_cast<const int4*>(kp.plan);
+    int4* dst = reinterpret_cast<int4*>(smem);
+    const int nv = kp.plan_bytes >> 4;
+    for (int q = tid; q < nv; q += blockDim.x) dst[q] = src[q];
+  }
+  __syncthreads();
+  const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(smem);
+  const Rec* recs = reinterpret_cast<const Rec*>(smem + sizeof(PlanHeader));
+  const int warp = tid >> 5, lane = tid & 31;
+  unsigned char* wbase = smem + kp.plan_bytes + warp * kp.ws_bytes;
+  const WsLayout L = ws_layout(P.n, P.S, P.pw_size, PREC == PHC_PREC_MIXED);
+  WarpWS ws;
+  ws.pwd = reinterpret_cast<cd*>(wbase + L.pwd);
+  ws.pwf = reinterpret_cast<cf*>(wbase + L.pwf);
+  ws.fvd = reinterpret_cast<cd*>(wbase + L.fvd);
+  ws.fvf = reinterpret_cast<cf*>(wbase + L.fvf);
+  ws.jd = reinterpret_cast<cd*>(wbase + L.jd);
+  ws.jf = reinterpret_cast<cf*>(wbase + L.jf);
+  ws.prow = reinterpret_cast<cd*>(wbase + L.prow);
+  WarpState& st = *reinterpret_cast<WarpState*>(wbase + L.st);
+  // structural zeros of the Jacobian are never written by the schedule
+  for (int q = lane; q < P.n * P.S; q += kWarp) {
+    sts(&ws.jd[q], czero<double>());
+    if (PREC == PHC_PREC_MIXED) sts(&ws.jf[q], czero<float>());
+  }
+  __syncwarp();
+  const int n = P.n, N = P.N;
+  // one call site of the path state machine: a persistent warp pulls paths
+  // from the atomic queue, a grid warp takes exactly one
+  long long q = -1, qend = 0;
+  for (;;) {
+    if (q + 1 < qend) {
+      ++q;
+    } else if (kp.persistent) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(kp.counter, (unsigned long long)kp.chunk);
+      base = __shfl_sync(kFull, base, 0);
+      if (base >= (unsigned long long)kp.count) break;
+      q = (long long)base;
+      qend = min((long long)base + kp.chunk, (long long)kp.count);
+    } else {
+      if (qend != 0) break;
+      q = (long long)blockIdx.x * kp.warps + warp;
+      qend = q + 1;
+      if (q >= kp.count) break;
+    }
+    track_one<NM, PREC>(P, recs, ws, st, kp.opts, kp.k0 + q, lane, kp.out + q,
+                        kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
+  }
+}
+
+}  // namespace phc
+
+// Host-side launch and occupancy helpers of one register-row width NM,
+// defined in the instantiation units track_nm*.cu.
+#define PHC_DEFINE_NM(NMV)                                                        \
+  namespace phc {                                                                 \
+  static void set_smem_attr_##NMV() {                                             \
+    static int done[64] = {0};                                                    \
+    int dev = 0;                                                                  \
+    cudaGetDevice(&dev);                                                          \
+    if (dev >= 0 && dev < 64 && !done[dev]) {                                     \
+      int smax = 0;                                                               \
+      cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev); \
+      cudaFuncSetAttribute(track_kernel<NMV, PHC_PREC_FP64>,                      \
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
+      cudaFuncSetAttribute(track_kernel<NMV, PHC_PREC_MIXED>,                     \
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
+      done[dev] = 1;                                                              \
+    }                                                                             \
+  }                                                                               \
+  cudaError_t launch_nm_##NMV(int prec, const KParams& kp, int grid, int block,   \
+                              int smem, cudaStream_t s) {                         \
+    set_smem_attr_##NMV();                                                        \
+    if (prec == PHC_PREC_MIXED)                                                   \
+      track_kernel<NMV, PHC_PREC_MIXED><<<grid, block, smem, s>>>(kp);            \
+    else                                                                          \
+      track_kernel<NMV, PHC_PREC_FP64><<<grid, block, smem, s>>>(kp);             \
+    return cudaGetLastError();                                                    \
+  }                                                                               \
+  int occupancy_nm_##NMV(int prec, int block, int smem) {                         \
+    set_smem_attr_##NMV();                                                        \
+    int nb = 0;                                                                   \
+    cudaError_t e =                                                               \
+        (prec == PHC_PREC_MIXED)                                                  \
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(                      \
+                  &nb, track_kernel<NMV, PHC_PREC_MIXED>, block, smem)            \
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(                      \
+                  &nb, track_kernel<NMV, PHC_PREC_FP64>, block, smem);            \
+    return e == cudaSuccess ? nb : 0;                                             \
+  }                                                                               \
+  }
