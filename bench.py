@@ -1,0 +1,378 @@
+"""Benchmark of the B200 path tracker on the batched-paths configuration:
+n = 10 variables, all degrees 2, 20 distinct monomials (of 66) per
+equation with complex normal coefficients, 1024 total-degree paths.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one pass of the tracker over all 1024 paths of the system
+(start_solution + track + Cauchy end game + classify numerics), i.e. the
+per-path work of one solve(). Metric: paths/s (higher is better).
+
+  value   mixed-precision persistent tracker, inputs (the compiled sparse
+          table) resident in device memory, timed with CUDA events on the
+          launching stream, L2 flushed (256 MiB written) between timed steps
+  e2e     the same metric through the public C ABI phc_solve_sparse (host
+          table in, host results out through page-locked buffers, host
+          bookkeeping included), wall clock per call
+  fp64    the plain all-FP64 tracker, one warp per path, no refill, same
+          timing as value (the baseline of the mixed-precision target)
+
+Under torchrun each rank solves its own system instance of the same shape
+(weak scaling, no collective on the data path); times are the max over
+ranks. --impl reference times the reference's CPU algorithm (the C++
+restatement under oracle/, all host threads) on the same workload.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "paths/s mixed vs FP64 at <=1e-10 endpoint err"
+WORKLOAD = ("batched paths: n=10, degrees 2, 20 of 66 monomials per equation, complex "
+            "normal coefficients, 1024 total-degree paths, end game on")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def workload(rank=0):
+    from polyhomocont_b200 import workloads as W
+    return W.cfg2(seed=W.seed_for(2, rank))
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the C++ restatement of the reference (oracle/), all threads
+# ---------------------------------------------------------------------------
+def cpu_paths_per_s(min_seconds=3.0, max_reps=50):
+    from oracle import oracle as O
+    from polyhomocont_b200 import workloads as W
+    O.build()
+    n, eqs = workload(0)
+    s = W.build(lambda: O.SparseSystem(fast=True), n, eqs)
+    threads = os.cpu_count() or 1
+    L = O.lib(fast=True)
+    npaths = int(L.orc_bezout(s.h))
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        O.solve_paths(s, nthreads=threads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or reps >= max_reps:
+            break
+    return npaths * reps / el, threads, f"all {npaths} paths x {reps} solves, {threads} threads", el
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from polyhomocont_b200 import workloads as W
+    O.build()
+    n, eqs = workload(0)
+    s = W.build(lambda: O.SparseSystem(fast=True), n, eqs)
+    threads = os.cpu_count() or 1
+    npaths = int(O.lib(fast=True).orc_bezout(s.h))
+    for _ in range(max(args.warmup, 0)):
+        O.solve_paths(s, nthreads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.solve_paths(s, nthreads=threads)
+    el = time.perf_counter() - t0
+    v = npaths * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "paths/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "paths": npaths, "threads": threads},
+        "cpu_baseline": {"value": v, "unit": "paths/s", "cores": threads, "kind": "port",
+                         "sample": f"all {npaths} paths per step, {threads} threads "
+                                   "(C++ restatement; no Fortran compiler for the reference)"},
+        "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    import torch
+    import polyhomocont_b200 as P
+    from polyhomocont_b200 import _abi, flops
+    from polyhomocont_b200 import workloads as W
+    from polyhomocont_b200 import build as B
+
+    if not os.path.exists(_abi.LIB_PATH):
+        B.build()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+        pg = dist
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    L = _abi.lib()
+    p64, p32 = ctypes.c_double(), ctypes.c_double()
+    st = L.phc_measure_fma_peaks(local, ctypes.byref(p64), ctypes.byref(p32))
+    if st != 0:
+        raise RuntimeError(f"phc_measure_fma_peaks: {_abi.last_error()}")
+    peak64, peak32 = p64.value, p32.value
+
+    n, eqs = workload(rank)
+    sysP = W.build(P.SparseSystem, n, eqs)
+    npaths = sysP.bezout()
+    t, _ = sysP.table()
+    T = sysP.total_terms()
+    hexps = np.ctypeslib.as_array(t.hexps, shape=(T * (n + 1),)).reshape(T, n + 1).copy()
+    model = flops.unit_model(n, sysP.degrees(), hexps)
+
+    g_mixed = P.default_gpu_options(P.PHC_PREC_MIXED, P.PHC_SCHED_PERSISTENT, device=local)
+    g_fp64 = P.default_gpu_options(P.PHC_PREC_FP64, P.PHC_SCHED_GRID, device=local)
+    plan_m = P.Plan(sysP, gpu=g_mixed)
+    plan_d = P.Plan(sysP, gpu=g_fp64)
+    out_m = torch.zeros(npaths * 96, dtype=torch.uint8, device=dev)
+    z_m = torch.zeros(npaths * (n + 1) * 2, dtype=torch.float64, device=dev)
+    out_d = torch.zeros_like(out_m)
+    z_d = torch.zeros_like(z_m)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def step(plan, out, z):
+        plan.launch(1, npaths, out.data_ptr(), z.data_ptr(), sptr)
+
+    def timed(plan, out, z, k):
+        total = 0.0
+        for _ in range(k):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(plan, out, z)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b) * 1e-3
+        return total
+
+    for _ in range(max(args.warmup, 3)):
+        step(plan_m, out_m, z_m)
+        step(plan_d, out_d, z_d)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    t_mixed = timed(plan_m, out_m, z_m, args.steps)
+    torch.cuda.synchronize()
+    barrier()
+    t_fp64 = timed(plan_d, out_d, z_d, args.steps)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    t_mixed_max = max_over_ranks(t_mixed)
+    t_fp64_max = max_over_ranks(t_fp64)
+
+    value = npaths * world * args.steps / t_mixed_max
+    v_fp64 = npaths * world * args.steps / t_fp64_max
+
+    # results of the last runs: counters for the flop model, endpoints
+    pm = np.frombuffer(out_m.cpu().numpy().tobytes(), dtype=P.PATH_DTYPE)
+    pd = np.frombuffer(out_d.cpu().numpy().tobytes(), dtype=P.PATH_DTYPE)
+    zm = z_m.cpu().numpy().view(np.complex128).reshape(npaths, n + 1)
+    zd = z_d.cpu().numpy().view(np.complex128).reshape(npaths, n + 1)
+    fin = (pd["status"] == 0) & (pd["at_infinity"] == 0)
+    err = 0.0
+    if fin.any():
+        xm = zm[fin, :n] / zm[fin, n:n + 1]
+        xd = zd[fin, :n] / zd[fin, n:n + 1]
+        err = float(np.max(np.max(np.abs(xm - xd), axis=1) /
+                           np.maximum(1.0, np.max(np.abs(xd), axis=1))))
+    same_class = all(np.array_equal(pm[k], pd[k]) for k in
+                     ("status", "winding_number", "at_infinity", "singular", "is_real"))
+    f64m, f32m = flops.path_flops(model, pm, mixed=True)
+    f64d, _ = flops.path_flops(model, pd, mixed=False)
+    per_launch_s = t_mixed / args.steps
+    achieved = (f64m + f32m) / per_launch_s / 1e12
+    t_at_peak = f64m / (peak64 * 1e12) + f32m / (peak32 * 1e12)
+    peak_eff = (f64m + f32m) / t_at_peak / 1e12 if t_at_peak > 0 else None
+    fp64_achieved = f64d / (t_fp64 / args.steps) / 1e12
+
+    # end to end through the public ABI
+    e2e = None
+    if not args.no_e2e:
+        def pinned(shape, dtype):
+            nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+            buf = torch.empty(max(nbytes, 1), dtype=torch.uint8, pin_memory=True)
+            arr = buf.numpy().view(dtype)[:int(np.prod(shape))].reshape(shape)
+            arr.fill(0)
+            pinned.keep.append(buf)
+            return arr
+        pinned.keep = []
+        bufs = P._result_buffers(n, npaths, alloc=pinned)
+        for _ in range(2):
+            P.solve(sysP, gpu=g_mixed, buffers=bufs)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            res, st = P.solve(sysP, gpu=g_mixed, buffers=bufs)
+        t_e2e = time.perf_counter() - t0
+        barrier()
+        t_e2e = max_over_ranks(t_e2e)
+        cfg = plan_m.config()
+        e2e = {"value": npaths * world * args.steps / t_e2e, "unit": "paths/s",
+               "h2d_bytes_per_step": cfg["table_bytes"],
+               "d2h_bytes_per_step": npaths * (96 + 16 * (n + 1) + 16 * n),
+               "ms_per_step": 1e3 * t_e2e / args.steps,
+               "nsolutions": int(res.nsolutions), "ninfinite": int(res.ninfinite),
+               "nfailed": int(res.nfailed)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, sample, el = cpu_paths_per_s()
+        cpu = {"value": v, "unit": "paths/s", "cores": cores, "kind": "port",
+               "sample": sample + " (C++ restatement of the reference, -O3)"}
+
+    if rank == 0:
+        cfg = plan_m.config()
+        line = {
+            "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_mixed_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (complex)",
+            "data": "synthetic (seeded reference generator)",
+            "config": {"workload": WORKLOAD, "paths": npaths, "precision": "mixed",
+                       "schedule": "persistent", "warps_per_block": cfg["warps_per_block"],
+                       "grid": cfg["grid"], "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"dp{world} (one system instance per GPU)"},
+            "fp64_plain": {"value": v_fp64, "unit": "paths/s",
+                           "ms_per_step": 1e3 * t_fp64_max / args.steps,
+                           "achieved_tflops": fp64_achieved,
+                           "frac_of_fp64_peak": fp64_achieved / peak64},
+            "mixed_vs_fp64": value / v_fp64,
+            "endpoint_max_rel_err_mixed_vs_fp64": err,
+            "classification_identical_mixed_vs_fp64": bool(same_class),
+            "roofline": {"bound": "fp64+fp32 CUDA-core pipes (no tensor cores, not HBM)",
+                         "achieved": achieved, "peak": peak_eff, "unit": "TFLOP/s",
+                         "frac": achieved / peak_eff if peak_eff else None,
+                         "traffic": None,
+                         "peak_fp64_tflops": peak64, "peak_fp32_tflops": peak32,
+                         "peak_source": "measured live (phc_measure_fma_peaks FMA loop)",
+                         "flops_per_launch": {"fp64": f64m, "fp32": f32m},
+                         "f_unit": model["F_unit"]},
+            "clocks": clocks,
+            "gpu_launches": args.steps,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    plan_m.close()
+    plan_d.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -144,7 +144,7 @@ typedef struct {
   int32_t n_refine;     /* refine units: evaluate + LU + solve            */
   int32_t n_eval;       /* evaluate-only units (backward error, classify) */
   int32_t n_cond;       /* cond1: LU + N solves                           */
-  int32_t n_fp64_retry; /* mixed: step attempts redone in FP64            */
+  int32_t n_fp64_retry; /* mixed: predictor/corrector units run in FP64   */
   double t;
   double endgame_error;
   double cond;
@@ -252,9 +252,10 @@ int32_t phc_plan_launch(phc_plan* plan, int64_t k0, int64_t count,
 /* number of kernel launches phc_plan_launch issues */
 int32_t phc_plan_launch_count(const phc_plan* plan);
 int32_t phc_plan_destroy(phc_plan* plan);
-/* resolved launch configuration of a plan */
+/* resolved launch configuration of a plan and the size of its device table */
 int32_t phc_plan_config(const phc_plan* plan, int32_t* warps_per_block,
-                        int32_t* grid, int32_t* smem_bytes, int32_t* unknowns_cap);
+                        int32_t* grid, int32_t* smem_bytes, int32_t* unknowns_cap,
+                        int32_t* table_bytes);
 
 /* ---- serving loop: continuous batching of whole systems ---------------- */
 typedef struct phc_server phc_server;
@@ -292,6 +293,9 @@ int32_t phc_server_destroy(phc_server* srv);
 const char* phc_version(void);
 /* last CUDA error text of this thread (after a PHC_ERR_CUDA return) */
 const char* phc_last_error(void);
+/* Measures the CUDA-core FP64 and FP32 FMA throughput of a device (TFLOP/s),
+ * the denominators of the tracker's roofline. Not part of the reference. */
+int32_t phc_measure_fma_peaks(int32_t device, double* fp64_tflops, double* fp32_tflops);
 
 #ifdef __cplusplus
 }

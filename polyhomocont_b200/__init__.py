@@ -150,17 +150,20 @@ class SolveResult:
         self.nduplicates = 0
 
 
-def _result_buffers(n, npaths):
+def _result_buffers(n, npaths, alloc=None):
+    """Host result arrays of one solve; alloc(shape, dtype) may provide
+    page-locked memory."""
+    alloc = alloc or (lambda shape, dtype: np.zeros(shape, dtype=dtype))
     m = max(npaths, 1)
     nn = max(n, 1)
     bufs = dict(
-        paths=np.zeros(m, dtype=PATH_DTYPE),
-        z=np.zeros((m, n + 1), dtype=np.complex128),
-        x=np.zeros((m, nn), dtype=np.complex128),
-        sols=np.zeros((m, nn), dtype=np.complex128),
-        realsols=np.zeros((m, nn)),
-        ssols=np.zeros((m, nn), dtype=np.complex128),
-        mult=np.zeros(m, dtype=np.int32),
+        paths=alloc((m,), PATH_DTYPE),
+        z=alloc((m, n + 1), np.complex128),
+        x=alloc((m, nn), np.complex128),
+        sols=alloc((m, nn), np.complex128),
+        realsols=alloc((m, nn), np.float64),
+        ssols=alloc((m, nn), np.complex128),
+        mult=alloc((m,), np.int32),
     )
     rc = _abi.SolveResultC()
     rc.paths = bufs["paths"].ctypes.data_as(ctypes.c_void_p)
@@ -194,10 +197,11 @@ def _fill_result(n, npaths, bufs, rc):
     return res
 
 
-def solve(sys, options=None, gpu=None):
+def solve(sys, options=None, gpu=None, buffers=None):
     """solve(sys, res, status, options), src/solve.f90:154-215, on the GPU.
     Returns (res, status); status is err_invalid_input for systems the
-    reference rejects. Device errors raise PhcError."""
+    reference rejects. Device errors raise PhcError. buffers: optional
+    (bufs, rc) from _result_buffers, reused across calls."""
     L = _abi.lib()
     o = options if options is not None else default_options()
     g = gpu if gpu is not None else default_gpu_options()
@@ -208,7 +212,7 @@ def solve(sys, options=None, gpu=None):
     npaths = int(L.phc_bezout(ctypes.byref(t)))
     if npaths < 1:
         return SolveResult(), ERR_INVALID_INPUT
-    bufs, rc = _result_buffers(n, npaths)
+    bufs, rc = buffers if buffers is not None else _result_buffers(n, npaths)
     st = L.phc_solve_sparse(ctypes.byref(t), ctypes.byref(o), ctypes.byref(g), ctypes.byref(rc))
     _check_device_status(st, "phc_solve_sparse")
     if st != PHC_OK:
@@ -297,10 +301,12 @@ class Plan:
             raise PhcError(st, "phc_plan_launch")
 
     def config(self):
-        w, g, s, nm = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        w, g, s, nm, tb = (ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(),
+                           ctypes.c_int32(), ctypes.c_int32())
         self._L.phc_plan_config(self.h, ctypes.byref(w), ctypes.byref(g), ctypes.byref(s),
-                                ctypes.byref(nm))
-        return dict(warps_per_block=w.value, grid=g.value, smem=s.value, nm=nm.value)
+                                ctypes.byref(nm), ctypes.byref(tb))
+        return dict(warps_per_block=w.value, grid=g.value, smem=s.value, nm=nm.value,
+                    table_bytes=tb.value)
 
     def close(self):
         if self.h:

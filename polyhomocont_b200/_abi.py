@@ -129,7 +129,7 @@ SIGNATURES = [
     ("phc_plan_launch", c_i32, [c_vp, c_i64, c_i64, c_vp, c_vp, c_vp]),
     ("phc_plan_launch_count", c_i32, [c_vp]),
     ("phc_plan_destroy", c_i32, [c_vp]),
-    ("phc_plan_config", c_i32, [c_vp, P(c_i32), P(c_i32), P(c_i32), P(c_i32)]),
+    ("phc_plan_config", c_i32, [c_vp, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32)]),
     ("phc_server_create", c_i32, [P(ServerConfig), P(c_vp)]),
     ("phc_server_submit", c_i32, [c_vp, P(SystemC), P(SolveOptions), P(c_u64)]),
     ("phc_server_poll", c_i32, [c_vp, c_u64, P(c_i32)]),
@@ -138,6 +138,7 @@ SIGNATURES = [
     ("phc_server_npaths", c_i64, [c_vp, c_u64]),
     ("phc_server_stats", c_i32, [c_vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)]),
     ("phc_server_destroy", c_i32, [c_vp]),
+    ("phc_measure_fma_peaks", c_i32, [c_i32, P(c_dbl), P(c_dbl)]),
 ]
 
 _LIB = None

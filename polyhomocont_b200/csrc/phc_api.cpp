@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -249,6 +250,8 @@ struct DeviceWS {
   bool ready = false;
   cudaStream_t stream = nullptr;
   DevBuf plan, out, z, x, counter;
+  unsigned char* stage = nullptr;  // pinned staging of the table upload
+  size_t stage_cap = 0;
 };
 DeviceWS g_ws[64];
 
@@ -293,8 +296,15 @@ static int run_paths_sync(const HostPlan& hp, const phc_solve_options& so,
   if ((st = W.z.ensure(nz)) != PHC_OK) return st;
   if ((st = W.x.ensure(nx)) != PHC_OK) return st;
   if ((st = W.counter.ensure(16)) != PHC_OK) return st;
-  PHC_CUDA(cudaMemcpyAsync(W.plan.p, hp.bytes.data(), hp.bytes.size(), cudaMemcpyHostToDevice,
-                           W.stream));
+  if (hp.bytes.size() > W.stage_cap) {
+    if (W.stage) cudaFreeHost(W.stage);
+    W.stage = nullptr;
+    W.stage_cap = 0;
+    PHC_CUDA(cudaMallocHost((void**)&W.stage, hp.bytes.size() * 2));
+    W.stage_cap = hp.bytes.size() * 2;
+  }
+  std::memcpy(W.stage, hp.bytes.data(), hp.bytes.size());
+  PHC_CUDA(cudaMemcpyAsync(W.plan.p, W.stage, hp.bytes.size(), cudaMemcpyHostToDevice, W.stream));
   KParams kp;
   std::memset(&kp, 0, sizeof(kp));
   kp.plan = static_cast<const unsigned char*>(W.plan.p);
@@ -336,26 +346,69 @@ static double norm_inf_c(const double* v, int n) {
   return r;
 }
 
-// find(x, pts, tol): first stored point within relative distance tol
-static int find_first(const double* x, const std::vector<double>& pts, int npts, int n,
-                      double tol) {
-  const double scale = std::max(1.0, norm_inf_c(x, n));
-  for (int j = 0; j < npts; ++j) {
-    const double* p = pts.data() + (size_t)j * 2 * n;
-    double d = 0.0;
-    for (int i = 0; i < n; ++i)
-      d = std::max(d, std::hypot(x[2 * i] - p[2 * i], x[2 * i + 1] - p[2 * i + 1]));
-    if (d <= tol * scale) return j + 1;
+// The reference's find (src/solve.f90:379-400) scans all stored points and
+// returns the first (lowest index) within tol * max(1, ||x||). PointSet
+// returns the same index without the O(P) scan: points are ordered by the
+// real part of their first coordinate, any match lies within the window
+// |Re x_1 - Re s_1| <= tol * max(1, ||x||), and the lowest index among the
+// matches in that window is the first match of the scan. Points or queries
+// with non-finite values take the linear scan, exactly as the reference.
+class PointSet {
+ public:
+  PointSet(int n, double tol) : n_(n), tol_(tol) {}
+  int size() const { return (int)(pts_.size() / (2 * (size_t)n_)); }
+  const std::vector<double>& data() const { return pts_; }
+
+  int find(const double* x) const {
+    const double scale = std::max(1.0, norm_inf_c(x, n_));
+    const double rho = tol_ * scale;
+    const double x0 = x[0];
+    int best = -1;
+    auto test = [&](int j) {
+      if (best >= 0 && j >= best) return;
+      if (within(x, j, rho)) best = j;
+    };
+    if (!std::isfinite(rho) || !std::isfinite(x0)) {
+      for (int j = 0; j < size(); ++j) test(j);
+    } else {
+      const double margin = 1e-12 * (std::fabs(x0) + rho) + 1e-300;
+      auto lo = ordered_.lower_bound(x0 - rho - margin);
+      auto hi = ordered_.upper_bound(x0 + rho + margin);
+      for (auto it = lo; it != hi; ++it) test(it->second);
+      for (int j : special_) test(j);
+    }
+    return best < 0 ? 0 : best + 1;
   }
-  return 0;
-}
+
+  void add(const double* x) {
+    const int j = size();
+    pts_.insert(pts_.end(), x, x + 2 * (size_t)n_);
+    if (std::isfinite(x[0]))
+      ordered_.emplace(x[0], j);
+    else
+      special_.push_back(j);
+  }
+
+ private:
+  bool within(const double* x, int j, double rho) const {
+    const double* p = pts_.data() + (size_t)j * 2 * n_;
+    double d = 0.0;
+    for (int i = 0; i < n_; ++i)
+      d = std::max(d, std::hypot(x[2 * i] - p[2 * i], x[2 * i + 1] - p[2 * i + 1]));
+    return d <= rho;
+  }
+  int n_;
+  double tol_;
+  std::vector<double> pts_;
+  std::multimap<double, int> ordered_;
+  std::vector<int> special_;
+};
 
 void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out* paths,
                  const double* x, phc_solve_result* res) {
   phc_solve_counts& c = res->counts;
-  std::vector<double> sols, ssols;
+  PointSet sols(n, o.dedup_tol), ssols(n, o.singular_dedup_tol);
   std::vector<int> mult;
-  int nsol = 0, nsing = 0;
   for (int64_t k = 0; k < npaths; ++k) {
     phc_path_out& p = paths[k];
     const double* xk = x + (size_t)k * 2 * n;
@@ -365,43 +418,45 @@ void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out
       c.nfailed++;
     } else if (p.at_infinity) {
       c.ninfinite++;
-    } else if (p.singular) {
-      int j = find_first(xk, ssols, nsing, n, o.singular_dedup_tol);
+    } else if (p.singular) {  // add_singular, src/solve.f90:353-377
+      int j = ssols.find(xk);
       if (j > 0) {
         mult[j - 1]++;
       } else {
-        ssols.insert(ssols.end(), xk, xk + 2 * n);
+        ssols.add(xk);
         mult.push_back(1);
-        j = ++nsing;
+        j = ssols.size();
       }
       p.singular_index = j;
-    } else {
-      int j = find_first(xk, sols, nsol, n, o.dedup_tol);
+    } else {  // add_solution, src/solve.f90:330-351
+      int j = sols.find(xk);
       if (j > 0) {
         c.nduplicates++;
       } else {
-        sols.insert(sols.end(), xk, xk + 2 * n);
-        j = ++nsol;
+        sols.add(xk);
+        j = sols.size();
       }
       p.solution_index = j;
     }
   }
+  const int nsol = sols.size(), nsing = ssols.size();
   c.nsolutions = nsol;
   c.nsingular = nsing;
-  if (res->solutions && nsol) std::memcpy(res->solutions, sols.data(), sols.size() * sizeof(double));
+  if (res->solutions && nsol)
+    std::memcpy(res->solutions, sols.data().data(), sols.data().size() * sizeof(double));
   if (res->singular_solutions && nsing)
-    std::memcpy(res->singular_solutions, ssols.data(), ssols.size() * sizeof(double));
+    std::memcpy(res->singular_solutions, ssols.data().data(), ssols.data().size() * sizeof(double));
   if (res->multiplicities)
     for (int j = 0; j < nsing; ++j) res->multiplicities[j] = mult[j];
   // collect_real, src/solve.f90:402-426
   int nreal = 0;
   for (int j = 0; j < nsol; ++j) {
-    const double* s = sols.data() + (size_t)j * 2 * n;
+    const double* sj = sols.data().data() + (size_t)j * 2 * n;
     double imax = 0.0;
-    for (int i = 0; i < n; ++i) imax = std::max(imax, std::fabs(s[2 * i + 1]));
-    if (imax <= o.real_tol * std::max(1.0, norm_inf_c(s, n))) {
+    for (int i = 0; i < n; ++i) imax = std::max(imax, std::fabs(sj[2 * i + 1]));
+    if (imax <= o.real_tol * std::max(1.0, norm_inf_c(sj, n))) {
       if (res->real_solutions)
-        for (int i = 0; i < n; ++i) res->real_solutions[(size_t)nreal * n + i] = s[2 * i];
+        for (int i = 0; i < n; ++i) res->real_solutions[(size_t)nreal * n + i] = sj[2 * i];
       ++nreal;
     }
   }
@@ -665,8 +720,9 @@ int32_t phc_plan_launch(phc_plan* p, int64_t k0, int64_t count, phc_path_out* d_
 int32_t phc_plan_launch_count(const phc_plan* p) { return p ? 1 : 0; }
 
 int32_t phc_plan_config(const phc_plan* p, int32_t* warps, int32_t* grid, int32_t* smem,
-                        int32_t* nm) {
+                        int32_t* nm, int32_t* table_bytes) {
   if (!p) return PHC_ERR_BAD_HANDLE;
+  if (table_bytes) *table_bytes = (int32_t)p->hp.bytes.size();
   if (warps) *warps = p->cfg.warps;
   if (grid) *grid = p->cfg.grid;
   if (smem) *smem = p->cfg.smem;

@@ -90,6 +90,43 @@ __device__ __forceinline__ cpx<T> cdiv(cpx<T> a, cpx<T> b) {
   T den = b.im * ratio + b.re;
   return mkc<T>((a.im * ratio + a.re) / den, (a.im - a.re * ratio) / den);
 }
+// Real reciprocal for the pivots: the hardware approximation (rcp.approx,
+// about 23 correct bits in double) refined by two Newton-Raphson steps
+// r <- r + r (1 - d r), which square the relative error each time
+// (Newton's method for f(r) = 1/r - d), leaving an error of about one unit
+// in the last place for d in [1e-290, 1e290].
+__device__ __forceinline__ double rcp_nr(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ float rcp_nr(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  const float e = fmaf(-d, r, 1.0f);
+  return fmaf(r, e, r);
+}
+// 1/a = conj(a)/|a|^2; Smith's division where |a|^2 would underflow or
+// overflow.
+__device__ __forceinline__ cd crcp(cd a) {
+  const double d = a.re * a.re + a.im * a.im;
+  if (d >= 1e-290 && d <= 1e290) {
+    const double r = rcp_nr(d);
+    return mkc<double>(a.re * r, -a.im * r);
+  }
+  return cdiv(cone<double>(), a);
+}
+__device__ __forceinline__ cf crcp(cf a) {
+  const float d = a.re * a.re + a.im * a.im;
+  if (d >= 1e-36f && d <= 1e36f) {
+    const float r = rcp_nr(d);
+    return mkc<float>(a.re * r, -a.im * r);
+  }
+  return cdiv(cone<float>(), a);
+}
 __device__ __forceinline__ double cabs(cd a) { return hypot(a.re, a.im); }
 __device__ __forceinline__ float cabs(cf a) { return hypotf(a.re, a.im); }
 
@@ -183,6 +220,41 @@ __device__ __forceinline__ int warp_argmax_first(double key, bool cand, double& 
   kmax = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
   return m ? __ffs(m) - 1 : -1;
 }
+// Pivot search in one reduction: the high word of |a|^2 (|a|^2 >= 0, so its
+// bit pattern orders like the value) with its low 5 bits replaced by
+// 31 - lane; the maximum is the largest key and, among keys equal in the
+// leading 15 mantissa bits, the lowest lane (the reference scans rows in
+// order and keeps the first maximum). kmax is the key part of the winner
+// (0 when every candidate is zero or tiny).
+__device__ __forceinline__ int pivot_lane(double key, bool cand, int lane, unsigned& kmax) {
+  const unsigned hi = (unsigned)((unsigned long long)__double_as_longlong(key) >> 32);
+  const unsigned v = cand ? ((hi & ~31u) | (31u - (unsigned)lane)) : 0u;
+  const unsigned m = __reduce_max_sync(kFull, v);
+  kmax = m & ~31u;
+  return 31 - (int)(m & 31u);
+}
+__device__ __forceinline__ int pivot_lane(float key, bool cand, int lane, unsigned& kmax) {
+  const unsigned b = __float_as_uint(key);
+  const unsigned v = cand ? ((b & ~31u) | (31u - (unsigned)lane)) : 0u;
+  const unsigned m = __reduce_max_sync(kFull, v);
+  kmax = m & ~31u;
+  return 31 - (int)(m & 31u);
+}
+// Coarse variant for pivoting: the key is the high word of |a|^2, so
+// candidates that agree in their leading 20 mantissa bits tie and the
+// lowest lane wins. Returns -1 with kmax = 0 when every candidate key is 0.
+__device__ __forceinline__ int warp_argmax_hi(double key, bool cand, unsigned& kmax) {
+  const unsigned hi = cand ? (unsigned)((unsigned long long)__double_as_longlong(key) >> 32) : 0u;
+  kmax = __reduce_max_sync(kFull, hi);
+  const unsigned m = __ballot_sync(kFull, cand && hi == kmax);
+  return m ? __ffs(m) - 1 : -1;
+}
+__device__ __forceinline__ int warp_argmax_hi(float key, bool cand, unsigned& kmax) {
+  const unsigned b = cand ? __float_as_uint(key) : 0u;
+  kmax = __reduce_max_sync(kFull, b);
+  const unsigned m = __ballot_sync(kFull, cand && b == kmax);
+  return m ? __ffs(m) - 1 : -1;
+}
 __device__ __forceinline__ int warp_argmax_first(float key, bool cand, float& kmax) {
   unsigned b = cand ? __float_as_uint(key) : 0u;
   unsigned mx = __reduce_max_sync(kFull, b);
@@ -193,239 +265,286 @@ __device__ __forceinline__ int warp_argmax_first(float key, bool cand, float& km
 
 // ---- per-warp workspace -------------------------------------------------------
 struct WarpWS {
-  cd* pwd;   // power table z_j^e, FP64
-  cf* pwf;   // power table, FP32 (mixed precision only)
-  cd* fvd;   // F^h values
-  cf* fvf;
-  cd* jd;    // Jacobian of F^h, row-major, stride S
+  cd* pwd;    // power table z_j^e, FP64
+  cf* pwf;    // power table, FP32 (mixed precision only)
+  cd* jd;     // Jacobian of F^h, row-major, stride S
   cf* jf;
-  cd* prow;  // pivot-row broadcast buffer (FP32 rows use it as cf*)
+  cd* prow;   // double-buffered pivot row (FP32 rows use it as cf*)
+  int* piv;   // pivot row (lane) of each column
+  cd* sink;   // per-lane scratch for the schedule's non-final stores
 };
 
 template <typename T> __device__ __forceinline__ cpx<T>* ws_pw(const WarpWS& w);
 template <> __device__ __forceinline__ cd* ws_pw<double>(const WarpWS& w) { return w.pwd; }
 template <> __device__ __forceinline__ cf* ws_pw<float>(const WarpWS& w) { return w.pwf; }
-template <typename T> __device__ __forceinline__ cpx<T>* ws_fv(const WarpWS& w);
-template <> __device__ __forceinline__ cd* ws_fv<double>(const WarpWS& w) { return w.fvd; }
-template <> __device__ __forceinline__ cf* ws_fv<float>(const WarpWS& w) { return w.fvf; }
 template <typename T> __device__ __forceinline__ cpx<T>* ws_j(const WarpWS& w);
 template <> __device__ __forceinline__ cd* ws_j<double>(const WarpWS& w) { return w.jd; }
 template <> __device__ __forceinline__ cf* ws_j<float>(const WarpWS& w) { return w.jf; }
+
+// Constants of the system held in registers for the lifetime of a warp. The
+// shared-memory table could alias the workspace that the evaluation writes,
+// so reading its fields inside the hot loops would reload them after every
+// store; these copies are loaded once.
+struct WarpConst {
+  int n, N, S, maxexp, len_j;
+  int n_levels;                // levels of extended power-table entries
+  const int32_t* level_off;    // shared memory: word ranges per level
+  const uint32_t* pre;         // shared memory: (triple, destination) words
+  int deg;          // d_lane (lane < n)
+  double inv_deg;   // 1/d_lane
+  cd b;             // b_lane
+  cd gamma;
+  const cd* coefd;  // Jacobian schedule arrays (shared memory)
+  const cf* coeff;
+  const uint2* meta;
+  const double (*patch)[2];
+};
+
+__device__ __forceinline__ WarpConst load_warp_const(const PlanHeader& P,
+                                                     const unsigned char* pb, int lane) {
+  WarpConst C;
+  C.n = P.n;
+  C.N = P.N;
+  C.S = P.S;
+  C.maxexp = P.maxexp;
+  C.len_j = P.len_j;
+  C.n_levels = P.n_levels;
+  C.level_off = P.level_off;
+  C.pre = reinterpret_cast<const uint32_t*>(pb + P.off_pre);
+  C.deg = lane < P.n ? P.deg[lane] : 1;
+  C.inv_deg = lane < P.n ? P.inv_deg[lane] : 1.0;  // lane n: patch row, no scaling
+  C.b = lane < P.n ? mkc<double>(P.b[lane][0], P.b[lane][1]) : czero<double>();
+  C.gamma = mkc<double>(P.gamma[0], P.gamma[1]);
+  C.coefd = reinterpret_cast<const cd*>(pb + P.off_jd);
+  C.coeff = reinterpret_cast<const cf*>(pb + P.off_jf);
+  C.meta = reinterpret_cast<const uint2*>(pb + P.off_jm);
+  C.patch = P.patch;
+  return C;
+}
+
+template <typename T> __device__ __forceinline__ const cpx<T>* wc_coef(const WarpConst& C);
+template <> __device__ __forceinline__ const cd* wc_coef<double>(const WarpConst& C) {
+  return C.coefd;
+}
+template <> __device__ __forceinline__ const cf* wc_coef<float>(const WarpConst& C) {
+  return C.coeff;
+}
 
 // ---- sparse evaluation ----------------------------------------------------
 // Power table of lane j's coordinate: pw[e*N + j] = z_j^e, e = 0..maxexp,
 // by repeated multiplication (src/sparse.f90:251-255).
 template <typename T>
-__device__ __forceinline__ void power_table(const PlanHeader& P, cpx<T>* pw, cpx<T> zj,
+__device__ __forceinline__ void power_table(const WarpConst& C, cpx<T>* pw, cpx<T> zj,
                                             int lane) {
-  if (lane < P.N) {
-    cpx<T> p = cone<T>();
-    sts(&pw[lane], p);
-    for (int e = 1; e <= P.maxexp; ++e) {
-      p = p * zj;
-      sts(&pw[e * P.N + lane], p);
+  const bool own = lane < C.N;
+  cpx<T> p = cone<T>();
+  if (own) sts(&pw[lane], p);
+  for (int e = 1; e <= C.maxexp; ++e) {
+    p = p * zj;
+    if (own) sts(&pw[e * C.N + lane], p);
+  }
+  // extended entries: products of three earlier entries, level by level
+  for (int L = 0; L < C.n_levels; ++L) {
+    __syncwarp();
+    const int w1 = C.level_off[L + 1];
+    for (int w = C.level_off[L] + 2 * lane; w < w1; w += 2 * kWarp) {
+      const uint32_t t = C.pre[w];
+      const cpx<T> v = lds(&pw[t & 0x3ffu]) * lds(&pw[(t >> 10) & 0x3ffu]) *
+                       lds(&pw[(t >> 20) & 0x3ffu]);
+      sts(&pw[C.pre[w + 1]], v);
     }
   }
 }
 
-// Runs one schedule: lane sums the contributions of its entries and stores
-// each sum once into out[dest].
+// Runs the Jacobian schedule: the lane sums the contributions of its
+// entries and stores each sum once into out[dest]. Record i of the lane is
+// slot i*32 + lane of the coefficient and metadata arrays (layout in
+// phc_internal.h). Every record multiplies exactly three table entries (an
+// unused factor is pw[0] = 1, exact) and records do not depend on each
+// other except through the running sum, so consecutive records overlap in
+// the pipeline.
 template <typename T>
-__device__ __forceinline__ void run_schedule(const Rec* recs, int rbeg, int rend,
-                                             const cpx<T>* pw, cpx<T>* out) {
+__device__ __forceinline__ void run_schedule(const cpx<T>* __restrict__ coef,
+                                             const uint2* __restrict__ meta, int len, int lane,
+                                             const cpx<T>* __restrict__ pw,
+                                             cpx<T>* __restrict__ out, cpx<T>* __restrict__ sink) {
+  // All lanes run len (the longest lane's count, a multiple of 4: shorter
+  // lanes read zero padding records). Records are processed four at a time:
+  // the loads of a batch are issued together, then the products, then the
+  // running sums. A store happens for every record, to the entry when the
+  // record is its last contribution, else to the lane's scratch slot, so the
+  // loop has no data-dependent branch.
   cpx<T> acc = czero<T>();
-  cpx<T> carry = czero<T>();
-  for (int r = rbeg; r < rend; ++r) {
-    const Rec& R = recs[r];
-    const uint4 meta = *reinterpret_cast<const uint4*>(&R.dest);  // dest..fac[5]
-    const unsigned flags = (meta.x >> 24) & 0xffu;
-    const unsigned nf = (meta.x >> 16) & 0xffu;
-    const unsigned dest = meta.x & 0xffffu;
-    cpx<T> v = (flags & kRecContIn) ? carry : mkc<T>((T)R.cre, (T)R.cim);
-    const unsigned f01 = meta.y, f23 = meta.z, f45 = meta.w;
-    if (nf > 0) v = v * lds(&pw[f01 & 0xffffu]);
-    if (nf > 1) v = v * lds(&pw[f01 >> 16]);
-    if (nf > 2) v = v * lds(&pw[f23 & 0xffffu]);
-    if (nf > 3) v = v * lds(&pw[f23 >> 16]);
-    if (nf > 4) v = v * lds(&pw[f45 & 0xffffu]);
-    if (nf > 5) v = v * lds(&pw[f45 >> 16]);
-    if (flags & kRecContOut) {
-      carry = v;
-      continue;
+  for (int i0 = 0; i0 < len; i0 += 4) {
+    uint2 m[4];
+    cpx<T> c[4], p0[4], p1[4], p2[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int slot = (i0 + u) * kWarp + lane;
+      m[u] = meta[slot];
+      c[u] = lds(&coef[slot]);
     }
-    acc = acc + v;
-    if (flags & kRecLast) {
-      sts(&out[dest], acc);
-      acc = czero<T>();
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const unsigned lo = m[u].x, hi = m[u].y;
+      p0[u] = lds(&pw[(lo >> 15) & 0x3ffu]);
+      p1[u] = lds(&pw[(lo >> 25) | ((hi & 7u) << 7)]);
+      p2[u] = lds(&pw[(hi >> 3) & 0x3ffu]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const cpx<T> v = (c[u] * p0[u]) * (p1[u] * p2[u]);
+      const unsigned lo = m[u].x;
+      const bool last = (lo >> 12) & kRecLast;
+      acc = acc + v;
+      sts(last ? &out[lo & 0x3ffu] : sink, acc);
+      acc = last ? czero<T>() : acc;
     }
   }
+}
+
+template <typename T> __device__ __forceinline__ const cpx<T>* plan_coef(
+    const unsigned char* pb, int off_d, int off_f);
+template <> __device__ __forceinline__ const cd* plan_coef<double>(const unsigned char* pb,
+                                                                   int off_d, int) {
+  return reinterpret_cast<const cd*>(pb + off_d);
+}
+template <> __device__ __forceinline__ const cf* plan_coef<float>(const unsigned char* pb, int,
+                                                                  int off_f) {
+  return reinterpret_cast<const cf*>(pb + off_f);
 }
 
 // Homotopy H(z,t) = gamma t G(z) + (1 - t) F^h(z) plus the patch row
-// (tdh_evaluate, src/homotopy.f90:188-231). Input: lane j holds z_j.
-// Output: lane i holds row i of H_z in a[], and h_i, ht_i.
-// TJ is the type of the Jacobian and of the row; f is evaluated in double
-// when f64 is set (Newton residuals), else in TJ.
-template <int NM, typename TJ>
-__device__ __forceinline__ void evaluate(const PlanHeader& P, const Rec* recs,
-                                         const WarpWS& ws, cd zl, cd t, int lane,
-                                         bool f64, cpx<TJ> (&a)[NM], cd& h, cd& ht) {
-  const int n = P.n, N = P.N, S = P.S;
-  // power tables
-  if (f64 || sizeof(TJ) == 8) power_table<double>(P, ws.pwd, zl, lane);
-  if (sizeof(TJ) == 4) power_table<TJ>(P, ws_pw<TJ>(ws), ccast<TJ>(zl), lane);
+// (tdh_evaluate, src/homotopy.f90:188-231), in precision T. Input: lane j
+// holds z_j. Output: lane i holds row i of H_z in a[] (zero beyond N),
+// and h_i, ht_i. F^h_i is obtained from row i of its Jacobian by Euler's
+// relation for homogeneous polynomials, F^h_i = (1/d_i) sum_j z_j dF^h_i/dz_j,
+// which needs no evaluation of its own.
+template <int NM, typename T>
+__device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, cd zl, cd t,
+                                         int lane, cpx<T> (&a)[NM], cd& h, cd& ht) {
+  const int n = C.n, N = C.N, S = C.S;
+  cpx<T>* pw = ws_pw<T>(ws);
+  power_table<T>(C, pw, ccast<T>(zl), lane);
   __syncwarp();
-  const Rec* rf = recs;
-  const Rec* rj = recs + P.nrec_f;
-  if (f64) {
-    run_schedule<double>(rf, P.lane_f[lane], P.lane_f[lane + 1], ws.pwd, ws.fvd);
-  } else {
-    run_schedule<TJ>(rf, P.lane_f[lane], P.lane_f[lane + 1], ws_pw<TJ>(ws),
-                     ws_fv<TJ>(ws));
-  }
-  run_schedule<TJ>(rj, P.lane_j[lane], P.lane_j[lane + 1], ws_pw<TJ>(ws), ws_j<TJ>(ws));
+  run_schedule<T>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws),
+                  reinterpret_cast<cpx<T>*>(ws.sink) + lane);
   __syncwarp();
 
-  const cd gamma = mkc<double>(P.gamma[0], P.gamma[1]);
-  const cd gt = gamma * t;
-  const cd omt = mkc<double>(1.0 - t.re, -t.im);
-  const cd w = shfl(zl, n);
-  h = czero<double>();
-  ht = czero<double>();
-  if (lane < n) {
-    const int i = lane;
-    const int d = P.deg[i];
-    const cd bi = mkc<double>(P.b[i][0], P.b[i][1]);
-    const cpx<TJ> omtT = ccast<TJ>(omt);
-    const cpx<TJ>* J = ws_j<TJ>(ws) + i * S;
+  const cpx<T> gamma = ccast<T>(C.gamma);
+  const cpx<T> tt = ccast<T>(t);
+  const cpx<T> gt = gamma * tt;
+  const cpx<T> omt = mkc<T>(T(1) - tt.re, -tt.im);
+  const cpx<T>* zrow = pw + N;  // z_j = pw[1*N + j]
+  // Every lane i <= n runs the same code on row i of the buffer: the
+  // Jacobian row of F^h_i (i < n) or the patch a (i = n); F^h_i follows from
+  // Euler's relation, F^h_i = (1/d_i) sum_j z_j dF^h_i/dz_j, and the patch
+  // row gives h_n = a . z - 1 (src/homotopy.f90:228-230).
+  const bool eq = lane < n;
+  const int row = lane < n ? lane : n;
+  const cpx<T>* Jr = ws_j<T>(ws) + row * S;
+  cpx<T> f0 = czero<T>(), f1 = czero<T>();
 #pragma unroll
-    for (int j = 0; j < NM; ++j) a[j] = (j < N) ? omtT * lds(&J[j]) : czero<TJ>();
-    if (f64 || sizeof(TJ) == 8) {
-      const cd zi = zl;
-      const cd zd1 = cpowi(zi, d - 1);
-      const cd wd1 = cpowi(w, d - 1);
-      const cd g = zd1 * zi - (bi * wd1) * w;
-      const cd f = lds(&ws.fvd[i]);
-      h = gt * g + omt * f;
-      ht = gamma * g - f;
-      const cpx<TJ> dg = ccast<TJ>(((double)d * gt) * zd1);
-      const cpx<TJ> dw = ccast<TJ>(((double)d * (gt * bi)) * wd1);
-#pragma unroll
-      for (int j = 0; j < NM; ++j) {
-        if (j == i) a[j] = a[j] + dg;
-        if (j == n) a[j] = a[j] - dw;
-      }
+  for (int j = 0; j < NM; ++j) {
+    if (j < N) {
+      const cpx<T> jij = lds(&Jr[j]);
+      if (j & 1)
+        f1 = f1 + jij * lds(&zrow[j]);
+      else
+        f0 = f0 + jij * lds(&zrow[j]);
+      a[j] = eq ? omt * jij : jij;
     } else {
-      const cpx<TJ> zi = ccast<TJ>(zl);
-      const cpx<TJ> wT = ccast<TJ>(w);
-      const cpx<TJ> biT = ccast<TJ>(bi);
-      const cpx<TJ> gtT = ccast<TJ>(gt);
-      const cpx<TJ> zd1 = cpowi(zi, d - 1);
-      const cpx<TJ> wd1 = cpowi(wT, d - 1);
-      const cpx<TJ> g = zd1 * zi - (biT * wd1) * wT;
-      const cpx<TJ> f = lds(&ws_fv<TJ>(ws)[i]);
-      h = ccast<double>(gtT * g + omtT * f);
-      ht = ccast<double>(ccast<TJ>(gamma) * g - f);
-      const cpx<TJ> dg = ((TJ)d * gtT) * zd1;
-      const cpx<TJ> dw = ((TJ)d * (gtT * biT)) * wd1;
-#pragma unroll
-      for (int j = 0; j < NM; ++j) {
-        if (j == i) a[j] = a[j] + dg;
-        if (j == n) a[j] = a[j] - dw;
-      }
+      a[j] = czero<T>();
     }
-  } else if (lane == n) {
-#pragma unroll
-    for (int j = 0; j < NM; ++j)
-      a[j] = (j < N) ? mkc<TJ>((TJ)P.patch[j][0], (TJ)P.patch[j][1]) : czero<TJ>();
-  } else {
-#pragma unroll
-    for (int j = 0; j < NM; ++j) a[j] = czero<TJ>();
   }
-  // patch row residual h_n = a . z - 1 (src/homotopy.f90:228)
-  cd pz = (lane < N) ? mkc<double>(P.patch[lane][0], P.patch[lane][1]) * zl
-                     : czero<double>();
-  const cd s = warp_csum(pz);
-  if (lane == n) h = mkc<double>(s.re - 1.0, s.im);
+  const cpx<T> f = (T)C.inv_deg * (f0 + f1);
+  // start system G_i = z_i^d - b_i w^d from the power table
+  const int dm1 = eq ? C.deg - 1 : 0;
+  const cpx<T> zd1 = lds(&pw[dm1 * N + row]);
+  const cpx<T> wd1 = lds(&pw[dm1 * N + n]);
+  const cpx<T> zi = lds(&zrow[row]);
+  const cpx<T> w = lds(&zrow[n]);
+  const cpx<T> bi = ccast<T>(C.b);
+  const cpx<T> g = zd1 * zi - (bi * wd1) * w;
+  const T dd = (T)C.deg;
+  const cpx<T> dg = eq ? (dd * gt) * zd1 : czero<T>();
+  const cpx<T> dw = eq ? (dd * (gt * bi)) * wd1 : czero<T>();
+#pragma unroll
+  for (int j = 0; j < NM; ++j) {
+    if (j == lane) a[j] = a[j] + dg;
+    if (j == n) a[j] = a[j] - dw;
+  }
+  cpx<T> hh = eq ? gt * g + omt * f : mkc<T>(f.re - T(1), f.im);
+  cpx<T> hht = eq ? gamma * g - f : czero<T>();
+  if (lane > n) {
+    hh = hht = czero<T>();
+#pragma unroll
+    for (int j = 0; j < NM; ++j) a[j] = czero<T>();
+  }
+  h = ccast<double>(hh);
+  ht = ccast<double>(hht);
 }
 
-// ---- LU with partial pivoting, lane i owns row i --------------------------
-// Factorizes the N x N matrix held row-wise in a[] (lu_factor,
-// src/linalg.f90:26-78) without moving rows: pstep records the step at
-// which a lane's row was chosen as pivot row (NM if never), piv packs the
-// pivot lane of each step (4 steps per word). Multipliers overwrite a[k] of
-// the eliminated rows, U stays in the pivot rows. Returns false for an
-// exactly zero pivot column (err_singular_matrix).
-template <int NM, typename T>
-__device__ __forceinline__ bool lu_rows(cpx<T> (&a)[NM], int N, int lane, int& pstep,
-                                        unsigned (&piv)[(NM + 3) / 4], cpx<T>* prow) {
-  pstep = NM;
-#pragma unroll
-  for (int q = 0; q < (NM + 3) / 4; ++q) piv[q] = 0u;
-  bool ok = true;
-  StaticFor<0, NM>::run([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    if (!ok || k >= N) return;
-    const bool cand = lane < N && pstep == NM;
-    T key = a[k].re * a[k].re + a[k].im * a[k].im;
-    T kmax;
-    int p = warp_argmax_first(key, cand, kmax);
-    if (!(kmax > T(0))) {
-      // zero or underflowed squares: decide with the modulus itself
-      T m = cand ? cabs(a[k]) : T(0);
-      p = warp_argmax_first(m, cand, kmax);
-      if (!(kmax > T(0))) {
-        ok = false;
-        return;
-      }
+// ---- Gauss-Jordan elimination with partial pivoting -----------------------
+// Solves A X = B for the N x N matrix A held row-wise (lane i owns row i)
+// and R right-hand-side columns (lane i holds row i of B in r[]). Rows are
+// never moved: at step k every lane's row is shifted left by one column, so
+// the column being eliminated is always a[0]. The pivot is the row of
+// largest |a_ik|^2 among the rows not pivoted yet (pivot_lane; ties go to
+// the lowest row as in the reference's first-maximum scan,
+// src/linalg.f90:51-58). Every lane computes the reciprocal of its own
+// candidate while the reduction runs; the pivot row, its right-hand side
+// and its reciprocal are broadcast with shuffles, and every other row,
+// pivoted before or not, subtracts m * (1/p) times it (Gauss-Jordan: no
+// back substitution). Pivot rows are never rescaled: at the end each lane
+// multiplies its right-hand side by the reciprocal of its own pivot, and
+// piv[k] is the lane that then holds row k of X. Returns false for an
+// exactly zero pivot column (err_singular_matrix of lu_factor).
+template <int NM, int R, typename T>
+__device__ __forceinline__ bool gauss_jordan(cpx<T> (&a)[NM], cpx<T> (&r)[R], int N, int lane,
+                                             int* piv) {
+  bool done = false;
+  int mystep = -1;
+  cpx<T> myrinv = czero<T>();
+  cpx<T> m0 = a[0];
+  for (int k = 0; k < N; ++k) {
+    const bool cand = lane < N && !done;
+    const T d2 = m0.re * m0.re + m0.im * m0.im;
+    unsigned kmax;
+    int p = pivot_lane(d2, cand, lane, kmax);
+    // speculative reciprocal, used by the pivot lane only
+    const T rd = rcp_nr(d2);
+    cpx<T> rinv = mkc<T>(m0.re * rd, -m0.im * rd);
+    if (kmax == 0u) {
+      // zero or tiny squares: decide with the modulus itself
+      T km;
+      p = warp_argmax_first(cand ? cabs(m0) : T(0), cand, km);
+      if (!(km > T(0))) return false;
     }
-    piv[k >> 2] |= (unsigned)p << (8 * (k & 3));
-    if (lane == p) {
-      pstep = k;
-#pragma unroll
-      for (int j = k; j < NM; ++j)
-        if (j < N) sts(&prow[j], a[j]);
+    const bool isp = (lane == p);
+    if (isp && !(d2 >= T(1e-36) && d2 <= T(1e36))) rinv = crcp(m0);  // |p|^2 out of range
+    if (isp) {
+      done = true;
+      mystep = k;
+      myrinv = rinv;
     }
-    __syncwarp();
-    if (cand && lane != p) {
-      const cpx<T> l = cdiv(a[k], lds(&prow[k]));
-      a[k] = l;
+    const cpx<T> rp = shfl(rinv, p);
+    // multiplier; the pivot row only shifts (l = 0)
+    const cpx<T> l = isp ? czero<T>() : m0 * rp;
+    // next pivot column first, so that the next reduction can start early
+    a[0] = a[1] - l * shfl(a[1], p);
+    m0 = a[0];
 #pragma unroll
-      for (int j = k + 1; j < NM; ++j)
-        if (j < N) a[j] = a[j] - l * lds(&prow[j]);
-    }
-    __syncwarp();
-  });
-  return ok;
-}
-
-// Solves A x = b with the factors from lu_rows (lu_solve,
-// src/linalg.f90:80-114). Lane i passes b_i; lane j returns x_j.
-template <int NM, typename T>
-__device__ __forceinline__ cpx<T> solve_rows(const cpx<T> (&a)[NM], int N, int lane,
-                                             int pstep, const unsigned (&piv)[(NM + 3) / 4],
-                                             cpx<T> b) {
-  // forward substitution in pivot order (unit lower triangle)
-  StaticFor<0, NM>::run([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    if (k >= N) return;
-    const int p = (piv[k >> 2] >> (8 * (k & 3))) & 0xff;
-    const cpx<T> bp = shfl(b, p);
-    if (pstep > k && lane < N) b = b - a[k] * bp;
-  });
-  // back substitution with U, last pivot first
-  cpx<T> x = czero<T>();
-  StaticFor<0, NM>::run([&](auto kc) {
-    constexpr int k = NM - 1 - decltype(kc)::value;
-    if (k >= N) return;
-    const int p = (piv[k >> 2] >> (8 * (k & 3))) & 0xff;
-    cpx<T> xk = czero<T>();
-    if (lane == p) xk = cdiv(b, a[k]);
-    xk = shfl(xk, p);
-    if (pstep < k) b = b - a[k] * xk;
-    if (lane == k) x = xk;
-  });
-  return x;
+    for (int j = 1; j + 1 < NM; ++j) a[j] = a[j + 1] - l * shfl(a[j + 1], p);
+    a[NM - 1] = czero<T>();
+#pragma unroll
+    for (int q = 0; q < R; ++q) r[q] = r[q] - l * shfl(r[q], p);
+  }
+#pragma unroll
+  for (int q = 0; q < R; ++q) r[q] = r[q] * myrinv;
+  if (mystep >= 0) piv[mystep] = lane;
+  __syncwarp();
+  return true;
 }
 
 }  // namespace phc

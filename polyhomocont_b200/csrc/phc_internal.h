@@ -27,40 +27,49 @@
 namespace phc {
 
 constexpr int kMaxN = 32;      // unknowns N = n + 1 (one lane per row)
-constexpr int kMaxFac = 6;     // power-table factors per record
-constexpr int kMaxPw = 1024;   // power-table entries (maxexp + 1) * N
+constexpr int kMaxFac = 3;     // power-table factors per record (longer products chain)
+constexpr int kMaxPw = 1024;   // power-table entries (maxexp + 1) * N, 10-bit indices
 constexpr int kWarp = 32;
 
-enum : uint8_t {
-  kRecLast = 1,     // last contribution of its entry: store the sum
-  kRecContIn = 2,   // continues the product of the previous record
-  kRecContOut = 4,  // product continues in the next record
+// Record metadata, packed into 64 bits:
+//   bits  0- 9  dest   i*S + j: Jacobian entry (row-major, odd stride S)
+//   bits 12-14  flags  kRecLast: last contribution of its entry
+//   bits 15-44  fac    three 10-bit offsets into the extended power table
+// A record contributes coef * pw[fac_0] * pw[fac_1] * pw[fac_2]; unused
+// factor slots point at pw[0] = z_0^0 = 1. Extended entries pw[pw_size + e]
+// hold products of three earlier entries (terms with more than three
+// nonzero exponents), computed level by level before the records run.
+enum : unsigned {
+  kRecLast = 1,
 };
+constexpr int kMaxLevels = 8;
 
-// One contribution: coef * prod_{q < nf} pw[fac[q]], pw[e*N + j] = z_j^e.
-struct alignas(16) Rec {
-  double cre;
-  double cim;
-  uint16_t dest;   // f: equation i; J: i*S + j (row-major, odd stride S)
-  uint8_t nf;
-  uint8_t flags;
-  uint16_t fac[kMaxFac];
-};
-static_assert(sizeof(Rec) == 32, "record must be 32 bytes");
-
+// Records are stored lane-interleaved: record i of lane l sits in slot
+// i * 32 + l of three arrays (FP64 coefficient, FP32 coefficient, metadata),
+// so the 32 lanes of a warp read consecutive 16-, 8- and 8-byte words
+// without shared-memory bank conflicts.
 struct alignas(16) PlanHeader {
   int32_t n;            // variables / equations
   int32_t N;            // unknowns n + 1
   int32_t S;            // row stride of the Jacobian buffer (odd)
   int32_t maxexp;       // largest homogenized exponent
-  int32_t pw_size;      // (maxexp + 1) * N
-  int32_t nrec_f;       // records of the f schedule
-  int32_t nrec_j;       // records of the Jacobian schedule
-  int32_t total_bytes;  // header + records (multiple of 16)
-  int32_t lane_f[kWarp + 1];
-  int32_t lane_j[kWarp + 1];
-  int32_t deg[kMaxN];
+  int32_t pw_size;      // (maxexp + 1) * N, plus n_pre extended entries in the table
+  int32_t len_f;        // slots per lane of the f schedule
+  int32_t len_j;        // slots per lane of the Jacobian schedule
+  int32_t total_bytes;  // header + arrays (multiple of 16)
+  int32_t off_fd, off_ff, off_fm;  // byte offsets of the f schedule arrays
+  int32_t off_jd, off_jf, off_jm;  // byte offsets of the Jacobian schedule arrays
+  int32_t nrec;         // records of both schedules
+  int32_t n_pre;        // extended power-table entries (products of three)
+  int32_t off_pre;      // byte offset of their packed factor triples (uint32)
+  int32_t n_levels;
+  int32_t level_off[kMaxLevels + 1];  // word ranges per level (2 words per entry)
+  int32_t pw_total;     // pw_size + n_pre: entries of the per-warp table
   int32_t pad0_[2];
+  int32_t cnt_f[kWarp]; // records of each lane
+  int32_t cnt_j[kWarp];
+  int32_t deg[kMaxN];
+  double inv_deg[kMaxN];    // 1/d_i (Euler's relation for F^h_i)
   int64_t radix[kMaxN];     // prod_{l < i} d_l (mixed-radix start index)
   int64_t nstart;           // Bezout number
   int64_t pad1_;
@@ -126,7 +135,7 @@ struct alignas(16) WarpState {
 // Per-warp shared-memory workspace layout (byte offsets from the warp's
 // base), shared by host (sizing) and device (addressing).
 struct WsLayout {
-  int pwd, pwf, fvd, fvf, jd, jf, prow, st, bytes;
+  int pwd, pwf, jd, jf, prow, piv, sink, st, bytes;
 };
 
 PHC_HD inline int align16(int x) { return (x + 15) & ~15; }
@@ -136,11 +145,11 @@ PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size, bool mixed) {
   int off = 0;
   L.pwd = off; off += align16(pw_size * 16);
   L.pwf = off; off += mixed ? align16(pw_size * 8) : 0;
-  L.fvd = off; off += kWarp * 16;
-  L.fvf = off; off += mixed ? kWarp * 8 : 0;
-  L.jd = off; off += align16(n * S * 16);
-  L.jf = off; off += mixed ? align16(n * S * 8) : 0;
-  L.prow = off; off += kWarp * 16;
+  L.jd = off; off += align16((n + 1) * S * 16);  // rows 0..n-1: dF^h, row n: patch
+  L.jf = off; off += mixed ? align16((n + 1) * S * 8) : 0;
+  L.prow = off; off += 2 * (kMaxN + 8) * 16;  // double-buffered pivot row, rhs, 1/pivot
+  L.piv = off; off += kWarp * 4;
+  L.sink = off; off += kWarp * 16;
   L.st = off; off += align16((int)sizeof(WarpState));
   L.bytes = off;
   return L;

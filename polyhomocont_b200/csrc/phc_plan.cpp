@@ -2,7 +2,9 @@
 // type(sparse_system), src/sparse.f90:31-48) and the homotopy constants
 // into the device table described in phc_internal.h.
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <map>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -19,46 +21,70 @@ struct Contribution {
   std::vector<int> fac;  // power-table offsets e*N + j
 };
 
-// Appends the records of one entry (its contributions in term order),
-// splitting products with more than kMaxFac factors into chained records.
-void emit_entry(const std::vector<Contribution>& cs, std::vector<Rec>& out) {
+struct PackedRec {
+  double cre, cim;
+  uint64_t meta;
+};
+
+uint64_t pack_meta(int dest, int nf, unsigned flags, const int* fac) {
+  uint64_t m = (uint64_t)(dest & 0x3ff) | ((uint64_t)(flags & 7) << 12);
+  // unused factor slots stay 0, i.e. point at pw[0] = z_0^0 = 1, so that
+  // every record multiplies three factors without branching
+  for (int q = 0; q < nf; ++q) m |= (uint64_t)(fac[q] & 0x3ff) << (15 + 10 * q);
+  return m;
+}
+
+// Appends the records of one entry (its contributions in term order);
+// every contribution has at most kMaxFac factors at this point.
+void emit_entry(const std::vector<Contribution>& cs, std::vector<PackedRec>& out) {
   for (size_t c = 0; c < cs.size(); ++c) {
     const Contribution& C = cs[c];
-    const bool last_contrib = (c + 1 == cs.size());
-    size_t pos = 0;
-    bool first_chunk = true;
-    do {
-      Rec r;
-      std::memset(&r, 0, sizeof(r));
-      r.cre = first_chunk ? C.cre : 0.0;
-      r.cim = first_chunk ? C.cim : 0.0;
-      r.dest = (uint16_t)C.dest;
-      const size_t take = std::min<size_t>(kMaxFac, C.fac.size() - pos);
-      r.nf = (uint8_t)take;
-      for (size_t q = 0; q < take; ++q) r.fac[q] = (uint16_t)C.fac[pos + q];
-      pos += take;
-      uint8_t flags = 0;
-      if (!first_chunk) flags |= kRecContIn;
-      if (pos < C.fac.size()) {
-        flags |= kRecContOut;
-      } else if (last_contrib) {
-        flags |= kRecLast;
-      }
-      r.flags = flags;
-      out.push_back(r);
-      first_chunk = false;
-    } while (pos < C.fac.size());
+    const unsigned flags = (c + 1 == cs.size()) ? kRecLast : 0u;
+    PackedRec r;
+    r.cre = C.cre;
+    r.cim = C.cim;
+    r.meta = pack_meta(C.dest, (int)C.fac.size(), flags, C.fac.data());
+    out.push_back(r);
   }
 }
 
-// Longest-processing-time assignment of entries to the 32 lanes; records
-// laid out lane by lane, entries of a lane in increasing entry order.
+// Products with more than three factors: the first three are replaced by an
+// extended power-table entry (shared between contributions with the same
+// triple) until three or fewer remain. Entries are grouped in levels; an
+// entry only uses table entries of lower levels.
+struct PreTable {
+  int base = 0;  // index of the first extended entry (pw_size)
+  std::map<std::array<int, 3>, int> index;
+  std::vector<std::array<int, 3>> entries;
+  std::vector<int> level;
+  int level_of(int f) const { return f >= base ? level[f - base] + 1 : 0; }
+  int intern(const std::array<int, 3>& t) {
+    auto it = index.find(t);
+    if (it != index.end()) return it->second;
+    const int e = base + (int)entries.size();
+    entries.push_back(t);
+    level.push_back(std::max(level_of(t[0]), std::max(level_of(t[1]), level_of(t[2]))));
+    index[t] = e;
+    return e;
+  }
+  void reduce(std::vector<int>& fac) {
+    while (fac.size() > (size_t)kMaxFac) {
+      std::array<int, 3> t = {fac[0], fac[1], fac[2]};
+      const int e = intern(t);
+      fac.erase(fac.begin(), fac.begin() + 3);
+      fac.insert(fac.begin(), e);
+    }
+  }
+};
+
+// Longest-processing-time assignment of entries to the 32 lanes; each lane
+// gets its entries in increasing entry order.
 void schedule(const std::vector<std::vector<Contribution>>& entries,
-              std::vector<Rec>& recs, int32_t lane_begin[kWarp + 1]) {
+              std::vector<std::vector<PackedRec>>& lanes) {
   const int ne = (int)entries.size();
   std::vector<long> cost(ne, 0);
   for (int e = 0; e < ne; ++e)
-    for (const auto& c : entries[e]) cost[e] += 2 + (long)c.fac.size();
+    for (const auto& c : entries[e]) cost[e] += 3 + (long)c.fac.size();
   std::vector<int> order(ne);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(),
@@ -73,13 +99,38 @@ void schedule(const std::vector<std::vector<Contribution>>& entries,
     load[best] += cost[e];
     lane_entries[best].push_back(e);
   }
-  recs.clear();
+  lanes.assign(kWarp, {});
   for (int l = 0; l < kWarp; ++l) {
-    lane_begin[l] = (int32_t)recs.size();
     std::sort(lane_entries[l].begin(), lane_entries[l].end());
-    for (int e : lane_entries[l]) emit_entry(entries[e], recs);
+    for (int e : lane_entries[l]) emit_entry(entries[e], lanes[l]);
   }
-  lane_begin[kWarp] = (int32_t)recs.size();
+}
+
+// Writes one schedule's lane-interleaved arrays at the given offsets.
+void store_schedule(const std::vector<std::vector<PackedRec>>& lanes, int len,
+                    unsigned char* base, int off_d, int off_f, int off_m, int32_t* cnt) {
+  double* cd = reinterpret_cast<double*>(base + off_d);
+  float* cf = reinterpret_cast<float*>(base + off_f);
+  uint64_t* cm = reinterpret_cast<uint64_t*>(base + off_m);
+  for (int l = 0; l < kWarp; ++l) {
+    cnt[l] = (int32_t)lanes[l].size();
+    for (int i = 0; i < len; ++i) {
+      const size_t slot = (size_t)i * kWarp + l;
+      PackedRec r{0.0, 0.0, 0};
+      if (i < (int)lanes[l].size()) r = lanes[l][i];
+      cd[2 * slot] = r.cre;
+      cd[2 * slot + 1] = r.cim;
+      cf[2 * slot] = (float)r.cre;
+      cf[2 * slot + 1] = (float)r.cim;
+      cm[slot] = r.meta;
+    }
+  }
+}
+
+size_t max_len(const std::vector<std::vector<PackedRec>>& lanes) {
+  size_t m = 0;
+  for (const auto& v : lanes) m = std::max(m, v.size());
+  return m;
 }
 
 }  // namespace
@@ -114,8 +165,10 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   if (hom == nullptr || hom->b == nullptr || hom->patch == nullptr) return PHC_ERR_INVALID_INPUT;
   const int n = sys->n, N = n + 1;
   if (N > kMaxN) return PHC_ERR_UNSUPPORTED;
-  int maxexp = 0;
+  // the power table also holds z_i^(d_i-1) and w^(d_i-1) of the start system
+  int maxexp = 1;
   for (size_t q = 0; q < (size_t)sys->nterms * N; ++q) maxexp = std::max(maxexp, sys->hexps[q]);
+  for (int i = 0; i < n; ++i) maxexp = std::max(maxexp, sys->deg[i] - 1);
   const int pw_size = (maxexp + 1) * N;
   if (pw_size > kMaxPw) return PHC_ERR_UNSUPPORTED;
   const int S = (N % 2 == 1) ? N : N + 1;
@@ -130,6 +183,7 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   int64_t radix = 1;
   for (int i = 0; i < n; ++i) {
     H.deg[i] = sys->deg[i];
+    H.inv_deg[i] = 1.0 / (double)sys->deg[i];
     H.radix[i] = radix;
     radix *= sys->deg[i];
     if (radix > (int64_t)INT32_MAX) return PHC_ERR_INVALID_INPUT;
@@ -147,19 +201,14 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
     H.patch[j][1] = hom->patch[2 * j + 1];
   }
 
-  // contributions per entry, in term order (eval_terms, src/sparse.f90:259-278)
-  std::vector<std::vector<Contribution>> fent(n), jent((size_t)n * S);
+  // Jacobian contributions per entry, in term order (eval_terms,
+  // src/sparse.f90:259-278). F^h itself is not tabulated: the kernel
+  // obtains it from the Jacobian row by Euler's relation.
+  std::vector<std::vector<Contribution>> fent(0), jent((size_t)n * S);
   for (int i = 0; i < n; ++i) {
     for (int k = sys->first[i]; k < sys->first[i + 1]; ++k) {
       const int* e = sys->hexps + (size_t)k * N;
       const double cre = sys->coefs[2 * k], cim = sys->coefs[2 * k + 1];
-      Contribution v;
-      v.cre = cre;
-      v.cim = cim;
-      v.dest = i;
-      for (int j = 0; j < N; ++j)
-        if (e[j] > 0) v.fac.push_back(e[j] * N + j);
-      fent[i].push_back(v);
       for (int j = 0; j < N; ++j) {
         if (e[j] <= 0) continue;
         Contribution d;
@@ -173,27 +222,72 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
       }
     }
   }
-  std::vector<Rec> rf, rj;
-  schedule(fent, rf, H.lane_f);
-  schedule(jent, rj, H.lane_j);
-  H.nrec_f = (int32_t)rf.size();
-  H.nrec_j = (int32_t)rj.size();
-  const size_t bytes = sizeof(PlanHeader) + (rf.size() + rj.size()) * sizeof(Rec);
-  H.total_bytes = (int32_t)bytes;
-
-  out->bytes.resize(bytes);
+  PreTable pre;
+  pre.base = pw_size;
+  for (auto& ent : jent)
+    for (auto& c : ent) pre.reduce(c.fac);
+  const int n_pre = (int)pre.entries.size();
+  int n_levels = 0;
+  for (int l : pre.level) n_levels = std::max(n_levels, l + 1);
+  if (pw_size + n_pre > kMaxPw || n_levels > kMaxLevels) return PHC_ERR_UNSUPPORTED;
+  // extended entries in level order (their indices are fixed already, so
+  // the table lists (index, triple) per level)
+  std::vector<uint32_t> pre_packed;
+  H.n_pre = n_pre;
+  H.n_levels = n_levels;
+  H.pw_total = pw_size + n_pre;
+  for (int L = 0; L < n_levels; ++L) {
+    H.level_off[L] = (int32_t)pre_packed.size();
+    for (int e = 0; e < n_pre; ++e) {
+      if (pre.level[e] != L) continue;
+      const auto& t = pre.entries[e];
+      // 10 bits per factor + the 10-bit destination offset (e) in a second word
+      pre_packed.push_back((uint32_t)(t[0] & 0x3ff) | ((uint32_t)(t[1] & 0x3ff) << 10) |
+                           ((uint32_t)(t[2] & 0x3ff) << 20));
+      pre_packed.push_back((uint32_t)(pw_size + e));
+    }
+  }
+  H.level_off[n_levels] = (int32_t)pre_packed.size();
+  std::vector<std::vector<PackedRec>> lf, lj;
+  schedule(fent, lf);
+  schedule(jent, lj);
+  // lanes run the schedule in batches of four records
+  const int len_f = (int)((max_len(lf) + 3) & ~(size_t)3);
+  const int len_j = (int)((max_len(lj) + 3) & ~(size_t)3);
+  H.len_f = len_f;
+  H.len_j = len_j;
+  size_t off = sizeof(PlanHeader);
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 15) & ~(size_t)15;
+    return (int32_t)o;
+  };
+  const size_t sf = (size_t)len_f * kWarp, sj = (size_t)len_j * kWarp;
+  H.off_fd = take(sf * 16);
+  H.off_ff = take(sf * 8);
+  H.off_fm = take(sf * 8);
+  H.off_jd = take(sj * 16);
+  H.off_jf = take(sj * 8);
+  H.off_jm = take(sj * 8);
+  H.off_pre = take(pre_packed.size() * 4);
+  H.total_bytes = (int32_t)off;
+  int nrec = 0;
+  for (const auto& v : lf) nrec += (int)v.size();
+  for (const auto& v : lj) nrec += (int)v.size();
+  H.nrec = nrec;
+  out->bytes.assign(off, 0);
+  store_schedule(lf, len_f, out->bytes.data(), H.off_fd, H.off_ff, H.off_fm, H.cnt_f);
+  store_schedule(lj, len_j, out->bytes.data(), H.off_jd, H.off_jf, H.off_jm, H.cnt_j);
+  if (!pre_packed.empty())
+    std::memcpy(out->bytes.data() + H.off_pre, pre_packed.data(), pre_packed.size() * 4);
   std::memcpy(out->bytes.data(), &H, sizeof(H));
-  if (!rf.empty()) std::memcpy(out->bytes.data() + sizeof(H), rf.data(), rf.size() * sizeof(Rec));
-  if (!rj.empty())
-    std::memcpy(out->bytes.data() + sizeof(H) + rf.size() * sizeof(Rec), rj.data(),
-                rj.size() * sizeof(Rec));
   out->n = n;
   out->N = N;
   out->S = S;
   out->maxexp = maxexp;
-  out->pw_size = pw_size;
+  out->pw_size = pw_size + n_pre;
   out->nstart = radix;
-  out->nrec = H.nrec_f + H.nrec_j;
+  out->nrec = nrec;
   return PHC_OK;
 }
 

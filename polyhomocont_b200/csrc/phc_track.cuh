@@ -6,9 +6,10 @@
 // cauchy_endgame inside endpoint) are flattened into one warp-uniform
 // state machine whose every step either changes control state or runs
 // exactly one "unit": an evaluation of H(z,t) (and H_z, H_t), optionally
-// followed by the LU factorization and one or N solves. There is a single
-// call site of the unit per precision, so the large unrolled LU/solve code
-// exists once per precision in the kernel binary, and the same machine
+// followed by a Gauss-Jordan solve (one right-hand side, or the columns of
+// the inverse for cond1). There is a single
+// call site of the unit per precision pair, so the elimination code exists
+// once per precision in the kernel binary, and the same machine
 // serves the predictor, the corrector, the end game's backward errors,
 // refine and cond1.
 #pragma once
@@ -17,6 +18,7 @@
 
 #include <cfloat>
 #include <cstdint>
+#include <type_traits>
 
 #include "phc_device.cuh"
 #include "phc_internal.h"
@@ -34,65 +36,69 @@ struct UnitRes {
   bool ok;    // LU nonsingular
 };
 
-// One unit in precision T (row/LU type). f64res selects FP64 evaluation of
-// F^h for the residual (always true when T is double).
-template <int NM, typename T>
-__device__ __forceinline__ void run_unit(const PlanHeader& P, const Rec* recs,
-                                         const WarpWS& ws, int kind, bool f64res, cd zin,
-                                         cd t, cd dt, int lane, UnitRes& u) {
-  cpx<T> a[NM];
+// One unit: evaluation in precision TE, elimination in precision TS.
+//   FP64 tracker:               TE = TS = double
+//   mixed predictor (tangent):  TE = TS = float
+//   mixed corrector (Newton):   TE = double (residual), TS = float
+template <int NM, typename TE, typename TS>
+__device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, int kind,
+                                         cd zin, cd t, cd dt, int lane, UnitRes& u) {
+  const int N = C.N;
+  cpx<TE> a[NM];
   cd h, ht;
-  evaluate<NM, T>(P, recs, ws, zin, t, lane, f64res || sizeof(T) == 8, a, h, ht);
-  const int N = P.N;
-  if (kind == UK_BACKERR) {
-    // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
-    // absolute row sum of H_z
-    double rs = 0.0;
+  evaluate<NM, TE>(C, ws, zin, t, lane, a, h, ht);
+  if constexpr (std::is_same<TE, double>::value && std::is_same<TS, double>::value) {
+    if (kind == UK_BACKERR) {
+      // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
+      // absolute row sum of H_z
+      double rs = 0.0;
 #pragma unroll
-    for (int j = 0; j < NM; ++j)
-      if (j < N) rs += (double)cabs(a[j]);
-    u.a1 = warp_max_nonneg(lane < N ? cabs(h) : 0.0);
-    u.a2 = warp_max_nonneg(lane < N ? rs : 0.0);
-    u.ok = true;
-    return;
-  }
-  double anorm = 0.0;
-  if (kind == UK_COND) {
-    // cond1, src/linalg.f90:135-174: ||A||_1 = largest column sum
-    u.h = h;
-#pragma unroll
-    for (int j = 0; j < NM; ++j) {
-      if (j < N) {
-        double c = warp_sum(lane < N ? (double)cabs(a[j]) : 0.0);
-        anorm = fmax(anorm, c);
-      }
+      for (int j = 0; j < NM; ++j) rs += cabs(a[j]);
+      u.a1 = warp_max_nonneg(lane < N ? cabs(h) : 0.0);
+      u.a2 = warp_max_nonneg(lane < N ? rs : 0.0);
+      u.ok = true;
+      return;
     }
-  }
-  int pstep;
-  unsigned piv[(NM + 3) / 4];
-  u.ok = lu_rows<NM, T>(a, N, lane, pstep, piv, reinterpret_cast<cpx<T>*>(ws.prow));
-  if (!u.ok) {
-    u.a1 = DBL_MAX;  // cond1 of an exactly singular matrix
-    return;
-  }
-  const int nsolve = (kind == UK_COND) ? N : 1;
-  const cd rhs0 = (kind == UK_TANGENT) ? -(ht * dt) : -h;
-  double ainv = 0.0;
-  for (int jj = 0; jj < nsolve; ++jj) {
-    cpx<T> rhs;
-    if (kind == UK_COND)
-      rhs = (lane == jj) ? cone<T>() : czero<T>();
-    else
-      rhs = ccast<T>(rhs0);
-    const cpx<T> x = solve_rows<NM, T>(a, N, lane, pstep, piv, rhs);
     if (kind == UK_COND) {
-      double s = warp_sum(lane < N ? (double)cabs(x) : 0.0);
-      ainv = fmax(ainv, s);
-    } else {
-      u.x = ccast<double>(x);
+      // cond1, src/linalg.f90:135-174: ||A||_1 ||A^-1||_1, the columns of
+      // A^-1 from Gauss-Jordan on [A | e_c0 .. e_c0+3]
+      u.h = h;
+      double anorm = 0.0;
+#pragma unroll
+      for (int j = 0; j < NM; ++j) {
+        if (j < N) anorm = fmax(anorm, warp_sum(lane < N ? cabs(a[j]) : 0.0));
+      }
+      constexpr int RC = 4;
+      double ainv = 0.0;
+      for (int c0 = 0; c0 < N; c0 += RC) {
+        if (c0 > 0) evaluate<NM, double>(C, ws, zin, t, lane, a, h, ht);
+        cd r[RC];
+#pragma unroll
+        for (int q = 0; q < RC; ++q) r[q] = (lane == c0 + q) ? cone<double>() : czero<double>();
+        if (!gauss_jordan<NM, RC, double>(a, r, N, lane, ws.piv)) {
+          u.a1 = DBL_MAX;  // cond1 of an exactly singular matrix
+          u.ok = false;
+          return;
+        }
+#pragma unroll
+        for (int q = 0; q < RC; ++q) {
+          if (c0 + q < N) ainv = fmax(ainv, warp_sum(lane < N ? cabs(r[q]) : 0.0));
+        }
+      }
+      u.a1 = anorm * ainv;
+      u.ok = true;
+      return;
     }
   }
-  if (kind == UK_COND) u.a1 = anorm * ainv;
+  cpx<TS> as[NM];
+#pragma unroll
+  for (int j = 0; j < NM; ++j) as[j] = ccast<TS>(a[j]);
+  cpx<TS> r[1];
+  r[0] = ccast<TS>((kind == UK_TANGENT) ? -(ht * dt) : -h);
+  u.ok = gauss_jordan<NM, 1, TS>(as, r, N, lane, ws.piv);
+  if (!u.ok) return;
+  const cpx<TS> x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
+  u.x = (lane < N) ? ccast<double>(x) : czero<double>();
 }
 
 enum Pc : int {
@@ -160,18 +166,38 @@ __device__ __forceinline__ cd seg_dt(const WarpState& st, double s) {  // :164-1
   return mkc<double>(0.0, st.seg_dth) * seg_t(st, s);
 }
 
+// t(s) and dt/ds together, with one sincos on arcs.
+__device__ __forceinline__ void seg_tdt(const WarpState& st, double s, cd& t, cd& dt) {
+  if (!st.seg_arc) {
+    t = seg_t(st, s);
+    dt = mkc<double>(st.seg_t1[0] - st.seg_t0[0], st.seg_t1[1] - st.seg_t0[1]);
+    return;
+  }
+  double sn, cs;
+  sincos(st.seg_th0 + s * st.seg_dth, &sn, &cs);
+  t = st.seg_r * mkc<double>(cs, sn);
+  dt = mkc<double>(0.0, st.seg_dth) * t;
+}
+
+// max_j |v_j|^2 over the warp (squared moduli compare like the moduli of
+// the reference's norm_inf, without a hypot per lane)
+__device__ __forceinline__ double vnorm2(cd v, int lane, int N) {
+  return warp_max_nonneg(lane < N ? v.re * v.re + v.im * v.im : 0.0);
+}
+
 #define LV(f) (reinterpret_cast<cd*>(st.f)[lane])
 #define LDV(f) lds(&LV(f))
 #define STV(f, v) sts(&LV(f), (v))
 
 // Tracks path k (1-based) and writes its record, z and x.
 template <int NM, int PREC>
-__device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, const WarpWS& ws,
-                          WarpState& st, const KOpts& O, int64_t k, int lane,
-                          phc_path_out* rec, double* zo, double* xo) {
+__device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& C,
+                                          const WarpWS& ws, WarpState& st, const KOpts& O,
+                                          int64_t k, int lane, phc_path_out* rec, double* zo,
+                                          double* xo) {
   const phc_tracker_options& TO = O.so.tracker;
   const phc_endgame_options& EO = O.so.endgame;
-  const int n = P.n, N = P.N;
+  const int n = C.n, N = C.N;
   constexpr bool kMixed = (PREC == PHC_PREC_MIXED);
 
   // hot lane vectors (component j in lane j)
@@ -182,7 +208,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, 
   bool att64 = true;
   // pending unit
   int uk = UK_TANGENT, pc_after = PC_FINISH;
-  bool u_f32 = false, u_f64res = true;
+  int u_prec = 0;  // 0: FP64, 1: FP32 evaluation + elimination, 2: FP64 evaluation + FP32 elimination
   cd tin = z, dtin = z;
   UnitRes U;
   U.x = U.h = czero<double>();
@@ -269,11 +295,9 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, 
           // predict_rk4 stage 1: tangent at (z, s), src/tracker.f90:283
           stage = 0;
           uk = UK_TANGENT;
-          u_f32 = !att64;
-          u_f64res = att64;
+          u_prec = att64 ? 0 : 1;
           zin = zs;
-          tin = seg_t(st, s);
-          dtin = seg_dt(st, s);
+          seg_tdt(st, s, tin, dtin);
           pc_after = PC_SEG_AFTER_UNIT;
           want = true;
           break;
@@ -308,16 +332,16 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, 
               if (stage < 3) {
                 ++stage;
                 uk = UK_TANGENT;
-                tin = seg_t(st, s_in);
-                dtin = seg_dt(st, s_in);
+                // stages 1 and 2 share s + ds/2: t and dt/ds are reused
+                if (stage != 2) seg_tdt(st, s_in, tin, dtin);
               } else {
                 // newton_correct at t(sn), src/tracker.f90:319-360
                 stage = 4;
                 dnorm_prev = kHuge;
                 uk = UK_NEWTON;
-                u_f64res = true;
+                u_prec = att64 ? 0 : 2;
                 zin = zp;
-                tin = seg_t(st, sn);
+                if (sn != s + ds) tin = seg_t(st, sn);  // else t(s + ds) of stage 3
               }
               pc_after = PC_SEG_AFTER_UNIT;
               want = true;
@@ -330,14 +354,15 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, 
               outcome = 2;
             } else {
               zp = zp + U.x;
-              const double dnorm = vnorm(U.x, lane, N);
-              const double znorm = vnorm(zp, lane, N);
-              if (dnorm <= TO.corrector_tol * znorm) {
+              // ||dz|| <= tol ||z|| and the contraction test on squared norms
+              const double d2 = vnorm2(U.x, lane, N);
+              const double z2 = vnorm2(zp, lane, N);
+              if (d2 <= (TO.corrector_tol * TO.corrector_tol) * z2) {
                 outcome = 1;
-              } else if (it > 1 && dnorm > TO.contraction * dnorm_prev) {
+              } else if (it > 1 && d2 > (TO.contraction * TO.contraction) * dnorm_prev) {
                 outcome = 2;
               } else {
-                dnorm_prev = dnorm;
+                dnorm_prev = d2;
                 if (it >= TO.corrector_maxit) {
                   outcome = 2;
                 } else {
@@ -367,14 +392,11 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, 
               // counting a rejection, and stay in FP64 for a few steps
               att64 = true;
               st.sticky = O.fp64_sticky;
-              ++st.c_retry;
               stage = 0;
               uk = UK_TANGENT;
-              u_f32 = false;
-              u_f64res = true;
+              u_prec = 0;
               zin = zs;
-              tin = seg_t(st, s);
-              dtin = seg_dt(st, s);
+              seg_tdt(st, s, tin, dtin);
               pc_after = PC_SEG_AFTER_UNIT;
               want = true;
               break;
@@ -608,8 +630,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, 
             err = vnorm(est - LDV(prev), lane, N) / fmax(vnorm(est, lane, N), kTiny);
           st.rec_err = err;
           uk = UK_BACKERR;
-          u_f32 = false;
-          u_f64res = true;
+          u_prec = 0;
           zin = est;
           tin = czero<double>();
           dtin = czero<double>();
@@ -656,8 +677,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, 
         // ---------------- classify, src/solve.f90:288-328 ---------------------
         case PC_CL_START:
           uk = UK_COND;
-          u_f32 = false;
-          u_f64res = true;
+          u_prec = 0;
           zin = z;
           tin = czero<double>();
           dtin = czero<double>();
@@ -793,10 +813,14 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const Rec* recs, 
       }
     }
     // ---- run the requested unit ----
-    if (kMixed && u_f32)
-      run_unit<NM, float>(P, recs, ws, uk, u_f64res, zin, tin, dtin, lane, U);
-    else
-      run_unit<NM, double>(P, recs, ws, uk, true, zin, tin, dtin, lane, U);
+    if (kMixed && u_prec == 1) {
+      run_unit<NM, float, float>(C, ws, uk, zin, tin, dtin, lane, U);
+    } else if (kMixed && u_prec == 2) {
+      run_unit<NM, double, float>(C, ws, uk, zin, tin, dtin, lane, U);
+    } else {
+      run_unit<NM, double, double>(C, ws, uk, zin, tin, dtin, lane, U);
+      if (kMixed && uk <= UK_NEWTON) ++st.c_retry;  // predictor/corrector unit in FP64
+    }
     ++st.units;
     pc = pc_after;
   }
@@ -818,23 +842,28 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
   }
   __syncthreads();
   const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(smem);
-  const Rec* recs = reinterpret_cast<const Rec*>(smem + sizeof(PlanHeader));
+  const unsigned char* recs = smem;  // header + lane-interleaved record arrays
   const int warp = tid >> 5, lane = tid & 31;
   unsigned char* wbase = smem + kp.plan_bytes + warp * kp.ws_bytes;
-  const WsLayout L = ws_layout(P.n, P.S, P.pw_size, PREC == PHC_PREC_MIXED);
+  const WsLayout L = ws_layout(P.n, P.S, P.pw_total, PREC == PHC_PREC_MIXED);
   WarpWS ws;
   ws.pwd = reinterpret_cast<cd*>(wbase + L.pwd);
   ws.pwf = reinterpret_cast<cf*>(wbase + L.pwf);
-  ws.fvd = reinterpret_cast<cd*>(wbase + L.fvd);
-  ws.fvf = reinterpret_cast<cf*>(wbase + L.fvf);
   ws.jd = reinterpret_cast<cd*>(wbase + L.jd);
   ws.jf = reinterpret_cast<cf*>(wbase + L.jf);
   ws.prow = reinterpret_cast<cd*>(wbase + L.prow);
+  ws.piv = reinterpret_cast<int*>(wbase + L.piv);
+  ws.sink = reinterpret_cast<cd*>(wbase + L.sink);
   WarpState& st = *reinterpret_cast<WarpState*>(wbase + L.st);
-  // structural zeros of the Jacobian are never written by the schedule
-  for (int q = lane; q < P.n * P.S; q += kWarp) {
-    sts(&ws.jd[q], czero<double>());
-    if (PREC == PHC_PREC_MIXED) sts(&ws.jf[q], czero<float>());
+  const WarpConst C = load_warp_const(P, smem, lane);
+  // structural zeros of the Jacobian are never written by the schedule;
+  // row n holds the patch a (the last row of H_z)
+  for (int q = lane; q < (P.n + 1) * P.S; q += kWarp) {
+    const int row = q / P.S, col = q - row * P.S;
+    cd v = czero<double>();
+    if (row == P.n && col < P.N) v = mkc<double>(P.patch[col][0], P.patch[col][1]);
+    sts(&ws.jd[q], v);
+    if (PREC == PHC_PREC_MIXED) sts(&ws.jf[q], ccast<float>(v));
   }
   __syncwarp();
   const int n = P.n, N = P.N;
@@ -857,7 +886,7 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
       qend = q + 1;
       if (q >= kp.count) break;
     }
-    track_one<NM, PREC>(P, recs, ws, st, kp.opts, kp.k0 + q, lane, kp.out + q,
+    track_one<NM, PREC>(P, C, ws, st, kp.opts, kp.k0 + q, lane, kp.out + q,
                         kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
   }
 }
