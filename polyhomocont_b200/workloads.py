@@ -34,7 +34,13 @@ def seed_for(cfg, sys_index=0):
 def monomials(n, dmax):
     """All exponent vectors of total degree <= dmax in n variables, in
     ascending lexicographic order of the exponent tuples."""
-    out = [e for e in itertools.product(range(dmax + 1), repeat=n) if sum(e) <= dmax]
+    out = []
+    for d in range(dmax + 1):
+        for combo in itertools.combinations_with_replacement(range(n), d):
+            e = [0] * n
+            for j in combo:
+                e[j] += 1
+            out.append(tuple(e))
     out.sort()
     return out
 
