@@ -239,6 +239,25 @@ int32_t phc_solve_paths(const phc_system* sys, const phc_homotopy* hom,
                         int64_t k0, int64_t count, phc_path_out* out,
                         double* z_out, double* x_out);
 
+/* Per-path numerics without any device allocation. No counterpart in the
+ * reference. For callers that cannot call cudaMalloc -- code that runs
+ * inside CUDA graph capture, services whose device memory is reserved up
+ * front, hosts that forbid device allocations after start-up. The caller
+ * passes the host table and constants and its own device output buffers
+ * (d_out[count], d_z[count][n+1][2], d_x[count][n][2] or NULL); the compiled
+ * table and the path-queue counter go into one fixed 256 KiB array in device
+ * memory that every GPU loading the library holds until exit. Tables larger
+ * than that are rejected with PHC_ERR_UNSUPPORTED. The call only enqueues
+ * work on `stream`; it calls no cudaMalloc, cudaFree or other allocating
+ * routine. Its first call on a device looks up the array's address on that
+ * device (make that first call before any stream capture). All calls share
+ * the array: calls that overlap on the GPU (different streams, no ordering)
+ * race on it; calls on one stream are ordered. */
+int32_t phc_solve_paths_noalloc(const phc_system* sys, const phc_homotopy* hom,
+                                const phc_solve_options* opts, const phc_gpu_options* gpu,
+                                int64_t k0, int64_t count, phc_path_out* d_out, double* d_z,
+                                double* d_x, void* stream);
+
 /* ---- device-resident plan (inputs already in device memory) ------------ */
 typedef struct phc_plan phc_plan;
 int32_t phc_plan_create(const phc_system* sys, const phc_homotopy* hom,

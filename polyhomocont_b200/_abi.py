@@ -124,6 +124,8 @@ SIGNATURES = [
                                  P(SolveResultC)]),
     ("phc_solve_paths", c_i32, [P(SystemC), P(HomotopyC), P(SolveOptions), P(GpuOptions),
                                 c_i64, c_i64, c_vp, P(c_dbl), P(c_dbl)]),
+    ("phc_solve_paths_noalloc", c_i32, [P(SystemC), P(HomotopyC), P(SolveOptions),
+                                        P(GpuOptions), c_i64, c_i64, c_vp, c_vp, c_vp, c_vp]),
     ("phc_plan_create", c_i32, [P(SystemC), P(HomotopyC), P(SolveOptions), P(GpuOptions),
                                 P(c_vp)]),
     ("phc_plan_launch", c_i32, [c_vp, c_i64, c_i64, c_vp, c_vp, c_vp]),
