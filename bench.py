@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serving-systems", type=int, default=4096,
+                    help="systems in the serving stream (0 skips the serving leg)")
     return ap.parse_args()
 
 
@@ -173,6 +175,55 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# serving: stream of random sparse systems (n ~ U{2..8}, d_i ~ U{2,3})
+# ---------------------------------------------------------------------------
+def serving(P, W, nsys, device, load=0.7):
+    systems = [W.build(P.SparseSystem, *W.stream_system(i)) for i in range(nsys)]
+    npaths = sum(s.bezout() for s in systems)
+    cfg = dict(device=device, nslots=8, max_batch_systems=64, max_batch_paths=1 << 15)
+
+    def drain(srv, tickets):
+        lat = []
+        for t in tickets:
+            srv.wait(t, 600000)
+            res, st, l = srv.result(t)
+            if st != 0:
+                raise RuntimeError(f"serving request failed with status {st}")
+            lat.append(l)
+        return np.asarray(lat)
+
+    # capacity: everything submitted at once
+    srv = P.Server(**cfg)
+    t0 = time.perf_counter()
+    tickets = [srv.submit(s)[0] for s in systems]
+    drain(srv, tickets)
+    cap = nsys / (time.perf_counter() - t0)
+    srv.close()
+    # Poisson arrivals at the given fraction of capacity
+    rate = load * cap
+    arrivals = W.poisson_arrivals(nsys, rate)
+    srv = P.Server(**cfg)
+    t0 = time.perf_counter()
+    tickets = []
+    for s, ta in zip(systems, arrivals):
+        now = time.perf_counter() - t0
+        if ta > now:
+            time.sleep(ta - now)
+        tickets.append(srv.submit(s)[0])
+    lat = drain(srv, tickets)
+    elapsed = time.perf_counter() - t0
+    stats = srv.stats()
+    srv.close()
+    return {"systems": nsys, "paths": npaths, "capacity_systems_per_s": cap,
+            "arrival_rate_per_s": rate, "load": load,
+            "systems_per_s": nsys / elapsed, "paths_per_s": npaths / elapsed,
+            "latency_p50_ms": 1e3 * float(np.percentile(lat, 50)),
+            "latency_p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "latency_max_ms": 1e3 * float(lat.max()), "batches": stats["batches"],
+            "slots": cfg["nslots"]}
 
 
 # ---------------------------------------------------------------------------
@@ -328,6 +379,10 @@ def main():
                "nsolutions": int(res.nsolutions), "ninfinite": int(res.ninfinite),
                "nfailed": int(res.nfailed)}
 
+    serve = None
+    if args.serving_systems > 0 and rank == 0:
+        serve = serving(P, W, args.serving_systems, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample, el = cpu_paths_per_s()
@@ -365,6 +420,7 @@ def main():
             "gpu_launches": args.steps,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "serving": serve,
         }
         print(json.dumps(line), flush=True)
     plan_m.close()

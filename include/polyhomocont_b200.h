@@ -231,6 +231,14 @@ int64_t phc_bezout(const phc_system* sys);
 int32_t phc_solve_sparse(const phc_system* sys, const phc_solve_options* opts,
                          const phc_gpu_options* gpu, phc_solve_result* res);
 
+/* The host half of solve() on per-path records produced elsewhere (e.g. by
+ * several GPUs on contiguous path ranges, gathered in path order):
+ * add_solution / add_singular / find / collect_real, src/solve.f90:193-213,
+ * :330-426. paths[npaths] gets its solution/singular indices; res arrays as
+ * for phc_solve_sparse (res->paths/z/x are not touched). */
+int32_t phc_finish_solve(int32_t n, int64_t npaths, const phc_solve_options* opts,
+                         phc_path_out* paths, const double* x, phc_solve_result* res);
+
 /* Per-path numerics only (start_solution + endpoint + classify) for the
  * 1-based paths k0 .. k0+count-1 of the homotopy hom; host buffers:
  * out[count], z_out[count][n+1][2], x_out[count][n][2] (x may be NULL). */

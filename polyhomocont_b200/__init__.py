@@ -379,3 +379,78 @@ def result_from_arrays(n, paths, x, options=None):
     res.nreal = len(reals)
     res.real_solutions = np.array(reals).reshape(len(reals), n)
     return res
+
+
+class Server:
+    """Serving loop with continuous batching (phc_server_*): requests are
+    whole solves; the library's engine thread admits them into batches as
+    slots (CUDA streams) and the device-memory budget free up, while other
+    batches are still running."""
+
+    def __init__(self, device=0, nslots=4, max_batch_systems=64, max_batch_paths=1 << 16,
+                 mem_budget_bytes=1 << 30, gpu=None):
+        self._L = _abi.lib()
+        cfg = _abi.ServerConfig()
+        cfg.device = device
+        cfg.nslots = nslots
+        cfg.max_batch_systems = max_batch_systems
+        cfg.max_batch_paths = max_batch_paths
+        cfg.mem_budget_bytes = mem_budget_bytes
+        cfg.gpu = gpu if gpu is not None else default_gpu_options(device=device)
+        self.h = ctypes.c_void_p()
+        st = self._L.phc_server_create(ctypes.byref(cfg), ctypes.byref(self.h))
+        if st != PHC_OK:
+            raise PhcError(st, "phc_server_create")
+        self.n_of = {}
+
+    def submit(self, sys, options=None):
+        """Returns (ticket, status); status != 0 means the request was refused
+        (err_invalid_input, PHC_ERR_ADMISSION, ...)."""
+        t, st = sys.table()
+        if st != PHC_OK:
+            return None, st
+        o = options if options is not None else default_options()
+        ticket = ctypes.c_uint64()
+        st = self._L.phc_server_submit(self.h, ctypes.byref(t), ctypes.byref(o),
+                                       ctypes.byref(ticket))
+        if st != PHC_OK:
+            return None, st
+        self.n_of[ticket.value] = sys.nvars()
+        return ticket.value, st
+
+    def poll(self, ticket):
+        done = ctypes.c_int32()
+        st = self._L.phc_server_poll(self.h, ctypes.c_uint64(ticket), ctypes.byref(done))
+        return st, bool(done.value)
+
+    def wait(self, ticket, timeout_ms=-1):
+        return self._L.phc_server_wait(self.h, ctypes.c_uint64(ticket), int(timeout_ms))
+
+    def result(self, ticket):
+        """(SolveResult, status, latency_s); releases the ticket."""
+        n = self.n_of.pop(ticket)
+        npaths = int(self._L.phc_server_npaths(self.h, ctypes.c_uint64(ticket)))
+        bufs, rc = _result_buffers(n, max(npaths, 1))
+        lat = ctypes.c_double()
+        st = self._L.phc_server_result(self.h, ctypes.c_uint64(ticket), ctypes.byref(rc),
+                                       ctypes.byref(lat))
+        if st != PHC_OK:
+            return None, st, lat.value
+        return _fill_result(n, npaths, bufs, rc), st, lat.value
+
+    def stats(self):
+        v = [ctypes.c_int64() for _ in range(4)]
+        self._L.phc_server_stats(self.h, *[ctypes.byref(x) for x in v])
+        return dict(submitted=v[0].value, completed=v[1].value, batches=v[2].value,
+                    in_flight=v[3].value)
+
+    def close(self):
+        if self.h:
+            self._L.phc_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -120,6 +120,8 @@ SIGNATURES = [
     ("phc_homotopy_init", c_i32, [P(SystemC), c_i32, P(c_dbl), P(c_dbl), P(c_dbl),
                                   P(c_i64)]),
     ("phc_bezout", c_i64, [P(SystemC)]),
+    ("phc_finish_solve", c_i32, [c_i32, c_i64, P(SolveOptions), c_vp, P(c_dbl),
+                                 P(SolveResultC)]),
     ("phc_solve_sparse", c_i32, [P(SystemC), P(SolveOptions), P(GpuOptions),
                                  P(SolveResultC)]),
     ("phc_solve_paths", c_i32, [P(SystemC), P(HomotopyC), P(SolveOptions), P(GpuOptions),

@@ -185,13 +185,13 @@ int homotopy_init(const phc_system* sys, int seed, HostHomotopy* h) {
 // ---------------------------------------------------------------------------
 // launch configuration
 // ---------------------------------------------------------------------------
-static int device_smem_optin(int device) {
+int device_smem_optin(int device) {
   int v = 0;
   if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess)
     return 48 * 1024;
   return v;
 }
-static int device_sms(int device) {
+int device_sms(int device) {
   int v = 0;
   if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 1;
   return v;
@@ -610,6 +610,17 @@ int32_t phc_solve_paths(const phc_system* sys, const phc_homotopy* hom,
   if (st != PHC_OK) return st;
   if (k0 + count - 1 > hp.nstart) return PHC_ERR_INVALID_INPUT;
   return run_paths_sync(hp, so, g, k0, count, out, z_out, x_out);
+}
+
+int32_t phc_finish_solve(int32_t n, int64_t npaths, const phc_solve_options* opts,
+                         phc_path_out* paths, const double* x, phc_solve_result* res) {
+  if (n < 1 || npaths < 0 || !res || (npaths > 0 && (!paths || !x))) return PHC_ERR_INVALID_INPUT;
+  const phc_solve_options so = opts ? *opts : solve_defaults();
+  std::memset(&res->counts, 0, sizeof(res->counts));
+  res->counts.n = n;
+  res->counts.npaths = (int32_t)npaths;
+  bookkeeping(n, npaths, so, paths, x, res);
+  return PHC_OK;
 }
 
 int32_t phc_solve_sparse(const phc_system* sys, const phc_solve_options* opts,

@@ -51,12 +51,19 @@ struct LaunchCfg {
   int smem = 0;        // dynamic shared memory per block
 };
 
+// Opt-in shared memory per block and SM count of a device (cached).
+int device_smem_optin(int device);
+int device_sms(int device);
 // Resolves the launch configuration for a plan on a device.
 int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, LaunchCfg* cfg);
 // Launches the tracking kernel (phc_kernels.cu).
 cudaError_t launch_track(const LaunchCfg& cfg, const KParams& kp, int grid, cudaStream_t s);
 // Occupancy (blocks per SM) of the kernel for a configuration.
 int track_blocks_per_sm(const LaunchCfg& cfg);
+// Batched kernel (many systems per launch) and its occupancy.
+cudaError_t launch_track_batch(int nm, int prec, int warps, int smem, const KParamsBatch& kb,
+                               int grid, cudaStream_t s);
+int track_batch_blocks_per_sm(int nm, int prec, int warps, int smem);
 
 KOpts make_kopts(const phc_solve_options& so, const phc_gpu_options& g);
 phc_gpu_options gpu_defaults();

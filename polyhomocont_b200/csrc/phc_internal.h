@@ -104,6 +104,38 @@ struct KParams {
   KOpts opts;
 };
 
+// One request of a batch (device memory): where its table, options and
+// outputs are (byte offsets into the batch buffer), and which global path
+// indices of the batch are its paths.
+struct alignas(16) BatchSys {
+  int64_t table_off;
+  int64_t path_begin;   // global index (0-based) of its first path in the batch
+  int64_t npaths;
+  int64_t out_off;      // phc_path_out[npaths]
+  int64_t z_off;        // double[npaths][N][2]
+  int64_t x_off;        // double[npaths][n][2], or -1
+  int32_t table_bytes;  // multiple of 16
+  int32_t pad_;
+  KOpts opts;
+};
+
+// Parameters of the batched kernel: persistent warps pull global path
+// indices of the whole batch from one queue; each warp stages the table and
+// options of the request it is working on into its own shared-memory slice
+// [table_cap | ws_cap | KOpts].
+struct KParamsBatch {
+  unsigned char* base;        // batch buffer: descriptors, tables, outputs
+  const BatchSys* sys;        // [nsys], sorted by path_begin
+  int32_t nsys;
+  int32_t chunk;              // paths per queue grab
+  int32_t table_cap;          // multiple of 16
+  int32_t ws_cap;             // multiple of 16
+  int32_t slice_bytes;        // table_cap + ws_cap + KOpts, multiple of 16
+  int32_t pad_;
+  int64_t total_paths;
+  unsigned long long* counter;
+};
+
 // Cold per-path state of the tracker state machine, kept in shared memory
 // (one per warp) so that registers stay free for the evaluation and the LU.
 // Scalars are warp-uniform; the vectors hold component j in slot j.

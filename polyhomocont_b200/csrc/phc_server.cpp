@@ -105,9 +105,9 @@ namespace phc {
 namespace {
 
 // Lays out a batch in one device buffer and one pinned buffer:
-// [plans | outputs(paths) | z | x], each request's region 256-aligned.
+// [descriptors | tables | outputs(paths) | z | x], regions 256-aligned.
 size_t layout_batch(std::vector<std::shared_ptr<Request>>& b) {
-  size_t off = 0;
+  size_t off = up256(b.size() * sizeof(BatchSys));
   for (auto& r : b) {
     r->off_plan = off;
     off += up256(r->plan.bytes.size());
@@ -151,52 +151,75 @@ int grow(Slot& s, size_t bytes, size_t ncounters) {
   return PHC_OK;
 }
 
+// One kernel per batch: every request's paths go into one queue, so small
+// systems share the GPU instead of running one after another. The register
+// capacity is the largest of the batch; each warp holds one table, one
+// workspace and one option block in its shared-memory slice.
 int launch_batch(phc_server* S, Slot& s) {
   const phc_gpu_options& g = S->cfg.gpu;
   size_t bytes = layout_batch(s.batch);
-  int st = grow(s, bytes, s.batch.size());
+  int st = grow(s, bytes, 1);
   if (st != PHC_OK) return st;
   s.bytes = bytes;
   unsigned char* dev = static_cast<unsigned char*>(s.dbuf);
-  size_t plan_end = 0;
-  for (auto& r : s.batch) {
-    std::memcpy(s.hbuf + r->off_plan, r->plan.bytes.data(), r->plan.bytes.size());
-    plan_end = std::max(plan_end, r->off_plan + up256(r->plan.bytes.size()));
-  }
-  cudaError_t e = cudaMemcpyAsync(dev, s.hbuf, plan_end, cudaMemcpyHostToDevice, s.stream);
-  if (e != cudaSuccess) return cuda_fail(e, "server H2D");
-  e = cudaMemsetAsync(s.counters, 0, s.batch.size() * sizeof(unsigned long long), s.stream);
-  if (e != cudaSuccess) return cuda_fail(e, "server counters reset");
+  const int prec = (g.precision == PHC_PREC_MIXED) ? PHC_PREC_MIXED : PHC_PREC_FP64;
+  int nm = 0, table_cap = 0, ws_cap = 0;
+  int64_t total = 0;
+  BatchSys* d = reinterpret_cast<BatchSys*>(s.hbuf);
+  size_t plan_end = up256(s.batch.size() * sizeof(BatchSys));
   for (size_t i = 0; i < s.batch.size(); ++i) {
     Request& r = *s.batch[i];
-    KParams kp;
-    std::memset(&kp, 0, sizeof(kp));
-    kp.plan = dev + r.off_plan;
-    kp.plan_bytes = align16((int)r.plan.bytes.size());
-    kp.ws_bytes = r.cfg.ws_bytes;
-    kp.warps = r.cfg.warps;
-    kp.persistent = r.cfg.persistent;
-    kp.chunk = r.cfg.chunk;
-    kp.k0 = 1;
-    kp.count = r.npaths;
-    kp.counter = s.counters + i;
-    kp.out = reinterpret_cast<phc_path_out*>(dev + r.off_out);
-    kp.z = reinterpret_cast<double*>(dev + r.off_z);
-    kp.x = reinterpret_cast<double*>(dev + r.off_x);
-    kp.opts = make_kopts(r.opts, g);
-    int grid;
-    if (r.cfg.persistent) {
-      const int64_t per = (int64_t)r.cfg.warps * r.cfg.chunk;
-      grid = (int)std::min<int64_t>(r.cfg.grid, (r.npaths + per - 1) / per);
-    } else {
-      grid = (int)((r.npaths + r.cfg.warps - 1) / r.cfg.warps);
-    }
-    e = launch_track(r.cfg, kp, grid, s.stream);
-    if (e != cudaSuccess) return cuda_fail(e, "server kernel launch");
+    const int tb = align16((int)r.plan.bytes.size());
+    std::memcpy(s.hbuf + r.off_plan, r.plan.bytes.data(), r.plan.bytes.size());
+    plan_end = std::max(plan_end, r.off_plan + up256(r.plan.bytes.size()));
+    std::memset(&d[i], 0, sizeof(BatchSys));
+    d[i].table_off = (int64_t)r.off_plan;
+    d[i].table_bytes = tb;
+    d[i].path_begin = total;
+    d[i].npaths = r.npaths;
+    d[i].out_off = (int64_t)r.off_out;
+    d[i].z_off = (int64_t)r.off_z;
+    d[i].x_off = (int64_t)r.off_x;
+    d[i].opts = make_kopts(r.opts, g);
+    total += r.npaths;
+    nm = std::max(nm, r.cfg.nm);
+    table_cap = std::max(table_cap, tb);
+    ws_cap = std::max(ws_cap, align16(r.cfg.ws_bytes));
   }
+  const int slice = table_cap + ws_cap + align16((int)sizeof(KOpts));
+  const int smax = device_smem_optin(S->cfg.device);
+  int warps = g.warps_per_block > 0 ? std::min(std::max(g.warps_per_block, 1), 8) : 4;
+  while (warps > 1 && warps * slice > smax) --warps;
+  if (warps * slice > smax) {
+    set_last_error("batch tables do not fit in shared memory");
+    return PHC_ERR_UNSUPPORTED;
+  }
+  const int smem = warps * slice;
+  int bps = track_batch_blocks_per_sm(nm, prec, warps, smem);
+  if (bps < 1) bps = 1;
+  if (g.blocks_per_sm > 0) bps = std::min(bps, g.blocks_per_sm);
+  KParamsBatch kb;
+  std::memset(&kb, 0, sizeof(kb));
+  kb.base = dev;
+  kb.sys = reinterpret_cast<const BatchSys*>(dev);
+  kb.nsys = (int32_t)s.batch.size();
+  kb.chunk = g.chunk > 0 ? g.chunk : 1;
+  kb.table_cap = table_cap;
+  kb.ws_cap = ws_cap;
+  kb.slice_bytes = slice;
+  kb.total_paths = total;
+  kb.counter = s.counters;
+  const int64_t per = (int64_t)warps * kb.chunk;
+  const int grid =
+      (int)std::min<int64_t>((int64_t)device_sms(S->cfg.device) * bps, (total + per - 1) / per);
+  cudaError_t e = cudaMemcpyAsync(dev, s.hbuf, plan_end, cudaMemcpyHostToDevice, s.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "server H2D");
+  e = cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long), s.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "server counter reset");
+  e = launch_track_batch(nm, prec, warps, smem, kb, grid, s.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "server kernel launch");
   // results of the whole batch in one copy
-  size_t res_begin = plan_end;
-  e = cudaMemcpyAsync(s.hbuf + res_begin, dev + res_begin, bytes - res_begin,
+  e = cudaMemcpyAsync(s.hbuf + plan_end, dev + plan_end, bytes - plan_end,
                       cudaMemcpyDeviceToHost, s.stream);
   if (e != cudaSuccess) return cuda_fail(e, "server D2H");
   e = cudaEventRecord(s.done, s.stream);
@@ -366,7 +389,7 @@ int32_t phc_server_submit(phc_server* S, const phc_system* sys, const phc_solve_
   r->npaths = r->hom.nstart;
   st = resolve_launch(r->plan, S->cfg.gpu, S->cfg.device, &r->cfg);
   if (st != PHC_OK) return st;
-  r->dev_bytes = up256(r->plan.bytes.size()) + up256((size_t)r->npaths * sizeof(phc_path_out)) +
+  r->dev_bytes = sizeof(BatchSys) + up256(r->plan.bytes.size()) + up256((size_t)r->npaths * sizeof(phc_path_out)) +
                  up256((size_t)r->npaths * (r->n + 1) * 16) + up256((size_t)r->npaths * r->n * 16);
   if (r->dev_bytes > (size_t)S->cfg.mem_budget_bytes) {
     set_last_error("request larger than the server's memory budget");

@@ -830,6 +830,40 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
 #undef LDV
 #undef STV
 
+// Workspace pointers of a warp inside its shared-memory region.
+template <int PREC>
+__device__ __forceinline__ WarpWS warp_workspace(const PlanHeader& P, unsigned char* wbase,
+                                                WarpState** st) {
+  const WsLayout L = ws_layout(P.n, P.S, P.pw_total, PREC == PHC_PREC_MIXED);
+  WarpWS ws;
+  ws.pwd = reinterpret_cast<cd*>(wbase + L.pwd);
+  ws.pwf = reinterpret_cast<cf*>(wbase + L.pwf);
+  ws.jd = reinterpret_cast<cd*>(wbase + L.jd);
+  ws.jf = reinterpret_cast<cf*>(wbase + L.jf);
+  ws.prow = reinterpret_cast<cd*>(wbase + L.prow);
+  ws.piv = reinterpret_cast<int*>(wbase + L.piv);
+  ws.sink = reinterpret_cast<cd*>(wbase + L.sink);
+  *st = reinterpret_cast<WarpState*>(wbase + L.st);
+  return ws;
+}
+
+// Structural zeros of the Jacobian are never written by the schedule, so
+// the buffer is cleared once per system; row n holds the patch a (the last
+// row of H_z).
+template <int PREC>
+__device__ __forceinline__ void init_jacobian_buffer(const PlanHeader& P, const WarpWS& ws,
+                                                     int lane) {
+  for (int q = lane; q < (P.n + 1) * P.S; q += kWarp) {
+    const int row = q / P.S, col = q - row * P.S;
+    cd v = czero<double>();
+    if (row == P.n && col < P.N) v = mkc<double>(P.patch[col][0], P.patch[col][1]);
+    sts(&ws.jd[q], v);
+    if (PREC == PHC_PREC_MIXED) sts(&ws.jf[q], ccast<float>(v));
+  }
+  __syncwarp();
+}
+
+// Single-system kernel: every block stages the table once for its warps.
 template <int NM, int PREC>
 __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -842,30 +876,11 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
   }
   __syncthreads();
   const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(smem);
-  const unsigned char* recs = smem;  // header + lane-interleaved record arrays
   const int warp = tid >> 5, lane = tid & 31;
-  unsigned char* wbase = smem + kp.plan_bytes + warp * kp.ws_bytes;
-  const WsLayout L = ws_layout(P.n, P.S, P.pw_total, PREC == PHC_PREC_MIXED);
-  WarpWS ws;
-  ws.pwd = reinterpret_cast<cd*>(wbase + L.pwd);
-  ws.pwf = reinterpret_cast<cf*>(wbase + L.pwf);
-  ws.jd = reinterpret_cast<cd*>(wbase + L.jd);
-  ws.jf = reinterpret_cast<cf*>(wbase + L.jf);
-  ws.prow = reinterpret_cast<cd*>(wbase + L.prow);
-  ws.piv = reinterpret_cast<int*>(wbase + L.piv);
-  ws.sink = reinterpret_cast<cd*>(wbase + L.sink);
-  WarpState& st = *reinterpret_cast<WarpState*>(wbase + L.st);
+  WarpState* stp;
+  const WarpWS ws = warp_workspace<PREC>(P, smem + kp.plan_bytes + warp * kp.ws_bytes, &stp);
   const WarpConst C = load_warp_const(P, smem, lane);
-  // structural zeros of the Jacobian are never written by the schedule;
-  // row n holds the patch a (the last row of H_z)
-  for (int q = lane; q < (P.n + 1) * P.S; q += kWarp) {
-    const int row = q / P.S, col = q - row * P.S;
-    cd v = czero<double>();
-    if (row == P.n && col < P.N) v = mkc<double>(P.patch[col][0], P.patch[col][1]);
-    sts(&ws.jd[q], v);
-    if (PREC == PHC_PREC_MIXED) sts(&ws.jf[q], ccast<float>(v));
-  }
-  __syncwarp();
+  init_jacobian_buffer<PREC>(P, ws, lane);
   const int n = P.n, N = P.N;
   // one call site of the path state machine: a persistent warp pulls paths
   // from the atomic queue, a grid warp takes exactly one
@@ -886,8 +901,72 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
       qend = q + 1;
       if (q >= kp.count) break;
     }
-    track_one<NM, PREC>(P, C, ws, st, kp.opts, kp.k0 + q, lane, kp.out + q,
+    track_one<NM, PREC>(P, C, ws, *stp, kp.opts, kp.k0 + q, lane, kp.out + q,
                         kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
+  }
+}
+
+// Batched kernel: the paths of many systems (different n, degrees and
+// options) in one launch. Persistent warps pull global path indices from
+// one queue; a warp that moves on to another system stages that system's
+// table and options into its own shared-memory slice.
+template <int NM, int PREC>
+__global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char* slice = smem + warp * kb.slice_bytes;
+  unsigned char* tbl = slice;
+  unsigned char* wbase = slice + kb.table_cap;
+  KOpts* opts = reinterpret_cast<KOpts*>(wbase + kb.ws_cap);
+  int cur = -1;
+  long long q = -1, qend = 0;
+  for (;;) {
+    if (q + 1 < qend) {
+      ++q;
+    } else {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(kb.counter, (unsigned long long)kb.chunk);
+      base = __shfl_sync(kFull, base, 0);
+      if (base >= (unsigned long long)kb.total_paths) break;
+      q = (long long)base;
+      qend = min((long long)base + kb.chunk, (long long)kb.total_paths);
+    }
+    // the request owning global path q (uniform binary search)
+    int lo = 0, hi = kb.nsys - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (kb.sys[mid].path_begin <= q)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const BatchSys& S = kb.sys[lo];
+    if (lo != cur) {
+      cur = lo;
+      __syncwarp();
+      const int4* src = reinterpret_cast<const int4*>(kb.base + S.table_off);
+      int4* dst = reinterpret_cast<int4*>(tbl);
+      for (int v = lane; v < (S.table_bytes >> 4); v += kWarp) dst[v] = src[v];
+      static_assert(sizeof(KOpts) % 8 == 0, "KOpts is copied in 8-byte words");
+      const unsigned long long* osrc = reinterpret_cast<const unsigned long long*>(&S.opts);
+      unsigned long long* odst = reinterpret_cast<unsigned long long*>(opts);
+      for (int v = lane; v < (int)(sizeof(KOpts) >> 3); v += kWarp) odst[v] = osrc[v];
+      __syncwarp();
+      WarpState* stp;
+      const WarpWS ws0 = warp_workspace<PREC>(*reinterpret_cast<const PlanHeader*>(tbl), wbase,
+                                              &stp);
+      init_jacobian_buffer<PREC>(*reinterpret_cast<const PlanHeader*>(tbl), ws0, lane);
+    }
+    const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(tbl);
+    WarpState* stp;
+    const WarpWS ws = warp_workspace<PREC>(P, wbase, &stp);
+    const WarpConst C = load_warp_const(P, tbl, lane);
+    const long long kl = q - S.path_begin;  // 0-based path of the request
+    const int n = P.n, N = P.N;
+    phc_path_out* out = reinterpret_cast<phc_path_out*>(kb.base + S.out_off) + kl;
+    double* z = reinterpret_cast<double*>(kb.base + S.z_off) + 2 * kl * N;
+    double* x = S.x_off >= 0 ? reinterpret_cast<double*>(kb.base + S.x_off) + 2 * kl * n : nullptr;
+    track_one<NM, PREC>(P, C, ws, *stp, *opts, kl + 1, lane, out, z, x);
   }
 }
 
@@ -908,6 +987,10 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
                            cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
       cudaFuncSetAttribute(track_kernel<NMV, PHC_PREC_MIXED>,                     \
                            cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
+      cudaFuncSetAttribute(track_batch_kernel<NMV, PHC_PREC_FP64>,                \
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
+      cudaFuncSetAttribute(track_batch_kernel<NMV, PHC_PREC_MIXED>,               \
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
       done[dev] = 1;                                                              \
     }                                                                             \
   }                                                                               \
@@ -919,6 +1002,26 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
     else                                                                          \
       track_kernel<NMV, PHC_PREC_FP64><<<grid, block, smem, s>>>(kp);             \
     return cudaGetLastError();                                                    \
+  }                                                                               \
+  cudaError_t launch_batch_nm_##NMV(int prec, const KParamsBatch& kb, int grid,     \
+                                    int block, int smem, cudaStream_t s) {       \
+    set_smem_attr_##NMV();                                                        \
+    if (prec == PHC_PREC_MIXED)                                                   \
+      track_batch_kernel<NMV, PHC_PREC_MIXED><<<grid, block, smem, s>>>(kb);      \
+    else                                                                          \
+      track_batch_kernel<NMV, PHC_PREC_FP64><<<grid, block, smem, s>>>(kb);       \
+    return cudaGetLastError();                                                    \
+  }                                                                               \
+  int occupancy_batch_nm_##NMV(int prec, int block, int smem) {                   \
+    set_smem_attr_##NMV();                                                        \
+    int nb = 0;                                                                   \
+    cudaError_t e =                                                               \
+        (prec == PHC_PREC_MIXED)                                                  \
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(                      \
+                  &nb, track_batch_kernel<NMV, PHC_PREC_MIXED>, block, smem)      \
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(                      \
+                  &nb, track_batch_kernel<NMV, PHC_PREC_FP64>, block, smem);      \
+    return e == cudaSuccess ? nb : 0;                                             \
   }                                                                               \
   int occupancy_nm_##NMV(int prec, int block, int smem) {                         \
     set_smem_attr_##NMV();                                                        \

@@ -1,0 +1,71 @@
+"""Path sharding across GPUs (one process per GPU).
+
+Paths of one system are independent (src/solve.f90:190-208), so a solve
+splits into contiguous path ranges, one per rank, with no collective on the
+data path: each rank tracks its range on its own GPU, the per-path records
+are gathered to rank 0 in global path order, and rank 0 runs the
+order-dependent host bookkeeping (phc_finish_solve), which makes the result
+identical to a single-GPU solve.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+
+
+def path_range(npaths, rank, world):
+    """Contiguous, balanced 1-based range (k0, count) of rank's paths."""
+    base, extra = divmod(int(npaths), int(world))
+    count = base + (1 if rank < extra else 0)
+    k0 = 1 + rank * base + min(rank, extra)
+    return k0, count
+
+
+def finish_solve(n, paths, x, options=None):
+    """Host bookkeeping on gathered records (phc_finish_solve)."""
+    from . import SolveResult, _fill_result, _result_buffers, default_options
+    L = _abi.lib()
+    o = options if options is not None else default_options()
+    npaths = len(paths)
+    bufs, rc = _result_buffers(n, npaths)
+    bufs["paths"][:npaths] = paths
+    bufs["x"][:npaths, :n] = x
+    st = L.phc_finish_solve(int(n), int(npaths), ctypes.byref(o),
+                            bufs["paths"].ctypes.data_as(ctypes.c_void_p),
+                            _abi.dptr(bufs["x"].view(np.float64)), ctypes.byref(rc))
+    if st != 0:
+        raise RuntimeError(f"phc_finish_solve: {st}")
+    res = _fill_result(n, npaths, bufs, rc)
+    return res
+
+
+def solve_sharded(sys, rank, world, group=None, options=None, gpu=None, runner=None):
+    """solve() over `world` ranks. runner(k0, count) -> (paths, z, x) tracks a
+    path range; by default the GPU (phc_solve_paths on this rank's device).
+    Returns the SolveResult on rank 0 and None elsewhere."""
+    import torch.distributed as dist
+    from . import default_gpu_options, default_options, solve_paths
+    o = options if options is not None else default_options()
+    npaths = sys.bezout()
+    n = sys.nvars()
+    k0, count = path_range(npaths, rank, world)
+    if runner is None:
+        g = gpu if gpu is not None else default_gpu_options(device=rank)
+        paths, z, x, st = solve_paths(sys, o, g, k0=k0, count=count)
+        if st != 0:
+            raise RuntimeError(f"solve_paths on rank {rank}: status {st}")
+    else:
+        paths, z, x = runner(k0, count)
+    parts = [None] * world if rank == 0 else None
+    dist.gather_object((k0, np.asarray(paths), np.asarray(z), np.asarray(x)), parts,
+                       dst=0, group=group)
+    if rank != 0:
+        return None
+    parts.sort(key=lambda p: p[0])
+    paths = np.concatenate([p[1] for p in parts])
+    z = np.concatenate([p[2] for p in parts])
+    x = np.concatenate([p[3] for p in parts])
+    res = finish_solve(n, paths, x, o)
+    res.z = z
+    return res
