@@ -183,7 +183,7 @@ class ClockSampler:
 def serving(P, W, nsys, device, load=0.7):
     systems = [W.build(P.SparseSystem, *W.stream_system(i)) for i in range(nsys)]
     npaths = sum(s.bezout() for s in systems)
-    cfg = dict(device=device, nslots=8, max_batch_systems=64, max_batch_paths=1 << 15)
+    cfg = dict(device=device, nslots=16, max_batch_systems=64, max_batch_paths=1 << 15)
 
     def drain(srv, tickets):
         lat = []

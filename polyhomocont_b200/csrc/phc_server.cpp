@@ -72,8 +72,7 @@ struct Slot {
   size_t dcap = 0;
   unsigned char* hbuf = nullptr;  // pinned: plans in, results out
   size_t hcap = 0;
-  unsigned long long* counters = nullptr;  // one queue head per request
-  size_t ccap = 0;
+  unsigned long long* counters = nullptr;  // queue head of the batch kernel
   std::vector<std::shared_ptr<Request>> batch;
   size_t bytes = 0;
   bool busy = false;
@@ -99,6 +98,7 @@ struct phc_server {
   int64_t submitted = 0, completed = 0, batches = 0;
   size_t mem_in_use = 0;
   int init_status = PHC_OK;
+  std::vector<void*> retired_host;  // outgrown pinned buffers
 };
 
 namespace phc {
@@ -123,30 +123,29 @@ size_t layout_batch(std::vector<std::shared_ptr<Request>>& b) {
   return off;
 }
 
-int grow(Slot& s, size_t bytes, size_t ncounters) {
+// Grows a slot's buffers geometrically without a device-wide
+// synchronisation: device memory is stream-ordered (cudaMallocAsync /
+// cudaFreeAsync on the slot's stream), and pinned buffers that are
+// outgrown are kept until the server is destroyed, since cudaFreeHost
+// would wait for the whole device.
+int grow(Slot& s, size_t bytes, std::vector<void*>& retired_host) {
   if (bytes > s.dcap) {
-    if (s.dbuf) cudaFree(s.dbuf);
+    const size_t want = std::max(bytes, s.dcap + s.dcap / 2);
+    if (s.dbuf) cudaFreeAsync(s.dbuf, s.stream);
     s.dbuf = nullptr;
     s.dcap = 0;
-    cudaError_t e = cudaMalloc(&s.dbuf, bytes);
-    if (e != cudaSuccess) return cuda_fail(e, "server cudaMalloc");
-    s.dcap = bytes;
+    cudaError_t e = cudaMallocAsync(&s.dbuf, want, s.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "server cudaMallocAsync");
+    s.dcap = want;
   }
   if (bytes > s.hcap) {
-    if (s.hbuf) cudaFreeHost(s.hbuf);
+    const size_t want = std::max(bytes, s.hcap + s.hcap / 2);
+    if (s.hbuf) retired_host.push_back(s.hbuf);
     s.hbuf = nullptr;
     s.hcap = 0;
-    cudaError_t e = cudaMallocHost((void**)&s.hbuf, bytes);
-    if (e != cudaSuccess) return cuda_fail(e, "server cudaMallocHost");
-    s.hcap = bytes;
-  }
-  if (ncounters > s.ccap) {
-    if (s.counters) cudaFree(s.counters);
-    s.counters = nullptr;
-    s.ccap = 0;
-    cudaError_t e = cudaMalloc((void**)&s.counters, ncounters * sizeof(unsigned long long));
-    if (e != cudaSuccess) return cuda_fail(e, "server counters");
-    s.ccap = ncounters;
+    cudaError_t e = cudaHostAlloc((void**)&s.hbuf, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) return cuda_fail(e, "server cudaHostAlloc");
+    s.hcap = want;
   }
   return PHC_OK;
 }
@@ -158,7 +157,7 @@ int grow(Slot& s, size_t bytes, size_t ncounters) {
 int launch_batch(phc_server* S, Slot& s) {
   const phc_gpu_options& g = S->cfg.gpu;
   size_t bytes = layout_batch(s.batch);
-  int st = grow(s, bytes, 1);
+  int st = grow(s, bytes, S->retired_host);
   if (st != PHC_OK) return st;
   s.bytes = bytes;
   unsigned char* dev = static_cast<unsigned char*>(s.dbuf);
@@ -358,7 +357,14 @@ int32_t phc_server_create(const phc_server_config* cfg, phc_server** out) {
     if (e != cudaSuccess) return cuda_fail(e, "server stream");
     e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
     if (e != cudaSuccess) return cuda_fail(e, "server event");
+    e = cudaMalloc((void**)&s.counters, sizeof(unsigned long long));
+    if (e != cudaSuccess) return cuda_fail(e, "server counter");
+    // initial buffers sized for a typical batch, grown on demand
+    int st = grow(s, (size_t)1 << 22, S->retired_host);
+    if (st != PHC_OK) return st;
   }
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "server setup");
   phc_server* raw = S.release();
   raw->engine = std::thread(engine_main, raw);
   *out = raw;
@@ -498,12 +504,14 @@ int32_t phc_server_destroy(phc_server* S) {
   cudaSetDevice(S->cfg.device);
   for (auto& s : S->slots) {
     if (s.stream) cudaStreamSynchronize(s.stream);
-    if (s.dbuf) cudaFree(s.dbuf);
+    if (s.dbuf) cudaFreeAsync(s.dbuf, s.stream);
+    if (s.stream) cudaStreamSynchronize(s.stream);
     if (s.hbuf) cudaFreeHost(s.hbuf);
     if (s.counters) cudaFree(s.counters);
     if (s.done) cudaEventDestroy(s.done);
     if (s.stream) cudaStreamDestroy(s.stream);
   }
+  for (void* h : S->retired_host) cudaFreeHost(h);
   delete S;
   return PHC_OK;
 }
