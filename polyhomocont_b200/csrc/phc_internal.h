@@ -155,6 +155,7 @@ struct alignas(16) WarpState {
   double r, rnew, best_resid, dprev, cest, cest_prev, eg_segstep, eg_error, eg_residual,
       eg_radius, rec_err;
   double lp_spacing, lp_floor, lp_dth;
+  double cond_anorm, cond_ainv;  // cond1 accumulated over right-hand-side chunks
   long long units;
   int seg_arc, o_grow, seg_cont;
   int p_status, p_wind, p_egs, p_nacc, p_nrej, p_atinf, p_sing, p_real;
@@ -162,6 +163,7 @@ struct alignas(16) WarpState {
   int max_loops, eg_status, eg_wind, eg_nacc, eg_nrej, cw, rec_cont, have_prev, gate;
   int lp_c, lp_j, lp_max, lp_nsamp, lp_cont, lp_ok;
   int rf_it, sticky;
+  int cond_c0, cond_ret;  // cond1: first column of the current chunk, state to return to
 };
 
 // Per-warp shared-memory workspace layout (byte offsets from the warp's

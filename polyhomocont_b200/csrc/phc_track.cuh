@@ -31,23 +31,36 @@ enum UnitKind : int { UK_TANGENT = 0, UK_NEWTON = 1, UK_BACKERR = 2, UK_COND = 3
 struct UnitRes {
   cd x;       // solution component of this lane
   cd h;       // residual component of this lane (UK_COND)
-  double a1;  // UK_BACKERR: ||h||_inf; UK_COND: cond1
-  double a2;  // UK_BACKERR: max row sum of |H_z|
+  double a1;  // UK_BACKERR: ||h||_inf; UK_COND: ||A||_1 (first chunk)
+  double a2;  // UK_BACKERR: max row sum of |H_z|; UK_COND: max column sum of the chunk of A^-1
   bool ok;    // LU nonsingular
 };
 
-// One unit: evaluation in precision TE, elimination in precision TS.
-//   FP64 tracker:               TE = TS = double
-//   mixed predictor (tangent):  TE = TS = float
-//   mixed corrector (Newton):   TE = double (residual), TS = float
-template <int NM, typename TE, typename TS>
-__device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, int kind,
-                                         cd zin, cd t, cd dt, int lane, UnitRes& u) {
+// Columns of A^-1 per cond1 unit.
+constexpr int kCondChunk = 4;
+
+// One unit: an evaluation of H, H_z and H_t followed by one elimination.
+// prec selects the arithmetic (only the FP64 form exists when MIXED is
+// false):
+//   0: FP64 evaluation and elimination (FP64 tracker, FP64 retries, the
+//      end game's backward errors, refine, cond1)
+//   1: FP32 evaluation and elimination (mixed predictor, tangent)
+//   2: FP64 evaluation, FP32 elimination (mixed corrector: the residual in
+//      FP64, the update in FP32)
+// Every piece of code -- the FP32 and FP64 evaluation, the FP32 and FP64
+// elimination -- appears once in the kernel, which keeps the instruction
+// footprint of the mixed kernel close to that of the FP64 kernel.
+// UK_COND eliminates against the unit vectors e_c0 .. e_c0+3 (cond1,
+// src/linalg.f90:135-174); the state machine runs one such unit per chunk.
+template <int NM, bool MIXED>
+__device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, int kind, int prec,
+                                         int c0, cd zin, cd t, cd dt, int lane, UnitRes& u) {
   const int N = C.N;
-  cpx<TE> a[NM];
   cd h, ht;
-  evaluate<NM, TE>(C, ws, zin, t, lane, a, h, ht);
-  if constexpr (std::is_same<TE, double>::value && std::is_same<TS, double>::value) {
+  cpx<float> as[NM];
+  if (!MIXED || prec != 1) {
+    cpx<double> a[NM];
+    evaluate<NM, double>(C, ws, zin, t, lane, a, h, ht);
     if (kind == UK_BACKERR) {
       // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
       // absolute row sum of H_z
@@ -60,45 +73,55 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
       return;
     }
     if (kind == UK_COND) {
-      // cond1, src/linalg.f90:135-174: ||A||_1 ||A^-1||_1, the columns of
-      // A^-1 from Gauss-Jordan on [A | e_c0 .. e_c0+3]
       u.h = h;
-      double anorm = 0.0;
+      if (c0 == 0) {
+        double anorm = 0.0;
 #pragma unroll
-      for (int j = 0; j < NM; ++j) {
-        if (j < N) anorm = fmax(anorm, warp_sum(lane < N ? cabs(a[j]) : 0.0));
+        for (int j = 0; j < NM; ++j) {
+          if (j < N) anorm = fmax(anorm, warp_sum(lane < N ? cabs(a[j]) : 0.0));
+        }
+        u.a1 = anorm;
       }
-      constexpr int RC = 4;
+      cd r[kCondChunk];
+#pragma unroll
+      for (int q = 0; q < kCondChunk; ++q)
+        r[q] = (lane == c0 + q) ? cone<double>() : czero<double>();
+      if (!gauss_jordan<NM, kCondChunk, double>(a, r, N, lane, ws.piv)) {
+        u.ok = false;  // cond1 of an exactly singular matrix
+        return;
+      }
       double ainv = 0.0;
-      for (int c0 = 0; c0 < N; c0 += RC) {
-        if (c0 > 0) evaluate<NM, double>(C, ws, zin, t, lane, a, h, ht);
-        cd r[RC];
 #pragma unroll
-        for (int q = 0; q < RC; ++q) r[q] = (lane == c0 + q) ? cone<double>() : czero<double>();
-        if (!gauss_jordan<NM, RC, double>(a, r, N, lane, ws.piv)) {
-          u.a1 = DBL_MAX;  // cond1 of an exactly singular matrix
-          u.ok = false;
-          return;
-        }
-#pragma unroll
-        for (int q = 0; q < RC; ++q) {
-          if (c0 + q < N) ainv = fmax(ainv, warp_sum(lane < N ? cabs(r[q]) : 0.0));
-        }
+      for (int q = 0; q < kCondChunk; ++q) {
+        if (c0 + q < N) ainv = fmax(ainv, warp_sum(lane < N ? cabs(r[q]) : 0.0));
       }
-      u.a1 = anorm * ainv;
+      u.a2 = ainv;
       u.ok = true;
       return;
     }
-  }
-  cpx<TS> as[NM];
+    if (!MIXED || prec == 0) {
+      cd r[1];
+      r[0] = (kind == UK_TANGENT) ? -(ht * dt) : -h;
+      u.ok = gauss_jordan<NM, 1, double>(a, r, N, lane, ws.piv);
+      if (!u.ok) return;
+      const cd x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
+      u.x = (lane < N) ? x : czero<double>();
+      return;
+    }
+    // mixed corrector: FP64 residual, FP32 update
 #pragma unroll
-  for (int j = 0; j < NM; ++j) as[j] = ccast<TS>(a[j]);
-  cpx<TS> r[1];
-  r[0] = ccast<TS>((kind == UK_TANGENT) ? -(ht * dt) : -h);
-  u.ok = gauss_jordan<NM, 1, TS>(as, r, N, lane, ws.piv);
-  if (!u.ok) return;
-  const cpx<TS> x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
-  u.x = (lane < N) ? ccast<double>(x) : czero<double>();
+    for (int j = 0; j < NM; ++j) as[j] = ccast<float>(a[j]);
+  } else {
+    evaluate<NM, float>(C, ws, zin, t, lane, as, h, ht);
+  }
+  if constexpr (MIXED) {
+    cpx<float> r[1];
+    r[0] = ccast<float>((kind == UK_TANGENT) ? -(ht * dt) : -h);
+    u.ok = gauss_jordan<NM, 1, float>(as, r, N, lane, ws.piv);
+    if (!u.ok) return;
+    const cpx<float> x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
+    u.x = (lane < N) ? ccast<double>(x) : czero<double>();
+  }
 }
 
 enum Pc : int {
@@ -127,6 +150,7 @@ enum Pc : int {
   PC_CL_COND2,
   PC_CL_AFTER_COND2,
   PC_CL_FINAL,
+  PC_COND_STEP,
   PC_FINISH,
 };
 
@@ -224,6 +248,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
   st.c_tan = st.c_new = st.c_ref = st.c_eval = st.c_cond = st.c_retry = 0;
   st.units = 0;
   st.sticky = 0;
+  st.cond_c0 = 0;
   STV(xv, czero<double>());
 
   int pc = PC_START;
@@ -681,9 +706,36 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           zin = z;
           tin = czero<double>();
           dtin = czero<double>();
-          pc_after = PC_CL_AFTER_COND1;
+          st.cond_c0 = 0;
+          st.cond_ret = PC_CL_AFTER_COND1;
+          pc_after = PC_COND_STEP;
           want = true;
           break;
+
+        // cond1 (src/linalg.f90:135-174) chunk by chunk: ||A||_1 from the
+        // first unit, the largest column sum of A^-1 over all chunks
+        case PC_COND_STEP: {
+          const int c0 = st.cond_c0;
+          if (c0 == 0) st.cond_anorm = U.a1;
+          if (!U.ok) {
+            U.a1 = kHuge;  // huge(1.0_wp) for an exactly singular matrix
+            pc = st.cond_ret;
+            break;
+          }
+          const double ainv = (c0 == 0) ? U.a2 : fmax(st.cond_ainv, U.a2);
+          st.cond_ainv = ainv;
+          if (c0 + kCondChunk < N) {
+            st.cond_c0 = c0 + kCondChunk;
+            uk = UK_COND;
+            pc_after = PC_COND_STEP;
+            want = true;
+            break;
+          }
+          U.a1 = st.cond_anorm * ainv;
+          U.ok = true;
+          pc = st.cond_ret;
+          break;
+        }
 
         case PC_CL_AFTER_COND1: {
           ++st.c_eval;
@@ -738,8 +790,11 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
 
         case PC_CL_COND2:
           uk = UK_COND;
+          u_prec = 0;
           zin = z;
-          pc_after = PC_CL_AFTER_COND2;
+          st.cond_c0 = 0;
+          st.cond_ret = PC_CL_AFTER_COND2;
+          pc_after = PC_COND_STEP;
           want = true;
           break;
 
@@ -813,14 +868,8 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
       }
     }
     // ---- run the requested unit ----
-    if (kMixed && u_prec == 1) {
-      run_unit<NM, float, float>(C, ws, uk, zin, tin, dtin, lane, U);
-    } else if (kMixed && u_prec == 2) {
-      run_unit<NM, double, float>(C, ws, uk, zin, tin, dtin, lane, U);
-    } else {
-      run_unit<NM, double, double>(C, ws, uk, zin, tin, dtin, lane, U);
-      if (kMixed && uk <= UK_NEWTON) ++st.c_retry;  // predictor/corrector unit in FP64
-    }
+    run_unit<NM, kMixed>(C, ws, uk, kMixed ? u_prec : 0, st.cond_c0, zin, tin, dtin, lane, U);
+    if (kMixed && u_prec == 0 && uk <= UK_NEWTON) ++st.c_retry;  // predictor/corrector unit in FP64
     ++st.units;
     pc = pc_after;
   }
