@@ -77,6 +77,15 @@ template <typename T>
 __device__ __forceinline__ cpx<T> operator*(T s, cpx<T> a) {
   return mkc<T>(s * a.re, s * a.im);
 }
+// a - l*b as four fused multiply-adds, two deep per component (the
+// separate product and subtraction take six operations, three deep).
+__device__ __forceinline__ double fma_(double x, double y, double z) { return fma(x, y, z); }
+__device__ __forceinline__ float fma_(float x, float y, float z) { return fmaf(x, y, z); }
+template <typename T>
+__device__ __forceinline__ cpx<T> cfms(cpx<T> a, cpx<T> l, cpx<T> b) {
+  return mkc<T>(fma_(-l.re, b.re, fma_(l.im, b.im, a.re)),
+                fma_(-l.re, b.im, fma_(-l.im, b.re, a.im)));
+}
 // Complex division by Smith's method (R. L. Smith, CACM 5 (1962) 435),
 // the range-reducing division of Fortran compilers.
 template <typename T>
@@ -532,13 +541,13 @@ __device__ __forceinline__ bool gauss_jordan(cpx<T> (&a)[NM], cpx<T> (&r)[R], in
     // multiplier; the pivot row only shifts (l = 0)
     const cpx<T> l = isp ? czero<T>() : m0 * rp;
     // next pivot column first, so that the next reduction can start early
-    a[0] = a[1] - l * shfl(a[1], p);
+    a[0] = cfms(a[1], l, shfl(a[1], p));
     m0 = a[0];
 #pragma unroll
-    for (int j = 1; j + 1 < NM; ++j) a[j] = a[j + 1] - l * shfl(a[j + 1], p);
+    for (int j = 1; j + 1 < NM; ++j) a[j] = cfms(a[j + 1], l, shfl(a[j + 1], p));
     a[NM - 1] = czero<T>();
 #pragma unroll
-    for (int q = 0; q < R; ++q) r[q] = r[q] - l * shfl(r[q], p);
+    for (int q = 0; q < R; ++q) r[q] = cfms(r[q], l, shfl(r[q], p));
   }
 #pragma unroll
   for (int q = 0; q < R; ++q) r[q] = r[q] * myrinv;
