@@ -180,6 +180,14 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # serving: stream of random sparse systems (n ~ U{2..8}, d_i ~ U{2,3})
 # ---------------------------------------------------------------------------
+# DRAM bytes (read + write) of one mixed-precision launch on this workload,
+# from `ncu --set full --clock-control none -k regex:track_kernel -c 2` of
+# `python bench.py --steps 2 --warmup 3 --no-e2e --no-cpu --serving-systems 0`
+# (profiles/track_kernel_n10_1024paths.md). The kernel is compute- and
+# latency-bound; its traffic is the table, the start data and the results.
+NCU_DRAM_BYTES_PER_LAUNCH = 158464
+
+
 def serving(P, W, nsys, device, load=0.7):
     systems = [W.build(P.SparseSystem, *W.stream_system(i)) for i in range(nsys)]
     npaths = sum(s.bezout() for s in systems)
@@ -279,7 +287,9 @@ def main():
     model = flops.unit_model(n, sysP.degrees(), hexps)
 
     g_mixed = P.default_gpu_options(P.PHC_PREC_MIXED, P.PHC_SCHED_PERSISTENT, device=local)
-    g_fp64 = P.default_gpu_options(P.PHC_PREC_FP64, P.PHC_SCHED_GRID, device=local)
+    # the all-FP64 tracker with the same persistent schedule: only the
+    # precision differs between the two arms
+    g_fp64 = P.default_gpu_options(P.PHC_PREC_FP64, P.PHC_SCHED_PERSISTENT, device=local)
     plan_m = P.Plan(sysP, gpu=g_mixed)
     plan_d = P.Plan(sysP, gpu=g_fp64)
     out_m = torch.zeros(npaths * 96, dtype=torch.uint8, device=dev)
@@ -411,7 +421,10 @@ def main():
             "roofline": {"bound": "fp64+fp32 CUDA-core pipes (no tensor cores, not HBM)",
                          "achieved": achieved, "peak": peak_eff, "unit": "TFLOP/s",
                          "frac": achieved / peak_eff if peak_eff else None,
-                         "traffic": None,
+                         "traffic": NCU_DRAM_BYTES_PER_LAUNCH,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                           "one --set full capture of this workload "
+                                           "(profiles/track_kernel_n10_1024paths.md)",
                          "peak_fp64_tflops": peak64, "peak_fp32_tflops": peak32,
                          "peak_source": "measured live (phc_measure_fma_peaks FMA loop)",
                          "flops_per_launch": {"fp64": f64m, "fp32": f32m},
