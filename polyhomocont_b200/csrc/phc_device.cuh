@@ -296,6 +296,7 @@ template <> __device__ __forceinline__ cf* ws_j<float>(const WarpWS& w) { return
 // store; these copies are loaded once.
 struct WarpConst {
   int n, N, S, maxexp, len_j;
+  int max_fac;                 // most factors of any Jacobian record
   int n_levels;                // levels of extended power-table entries
   const int32_t* level_off;    // shared memory: word ranges per level
   const uint32_t* pre;         // shared memory: (triple, destination) words
@@ -317,6 +318,7 @@ __device__ __forceinline__ WarpConst load_warp_const(const PlanHeader& P,
   C.S = P.S;
   C.maxexp = P.maxexp;
   C.len_j = P.len_j;
+  C.max_fac = P.max_fac;
   C.n_levels = P.n_levels;
   C.level_off = P.level_off;
   C.pre = reinterpret_cast<const uint32_t*>(pb + P.off_pre);
@@ -368,11 +370,14 @@ __device__ __forceinline__ void power_table(const WarpConst& C, cpx<T>* pw, cpx<
 // Runs the Jacobian schedule: the lane sums the contributions of its
 // entries and stores each sum once into out[dest]. Record i of the lane is
 // slot i*32 + lane of the coefficient and metadata arrays (layout in
-// phc_internal.h). Every record multiplies exactly three table entries (an
-// unused factor is pw[0] = 1, exact) and records do not depend on each
-// other except through the running sum, so consecutive records overlap in
-// the pipeline.
-template <typename T>
+// phc_internal.h). A record multiplies its coefficient by up to three table
+// entries; F is the most any record of the system uses (an unused factor
+// is pw[0] = 1, exact), so a system whose records all have at most one
+// factor -- every quadratic system -- runs the one-factor form, which
+// loads and multiplies a third of the factors. Records do not depend on
+// each other except through the running sum, so consecutive records
+// overlap in the pipeline.
+template <typename T, int F>
 __device__ __forceinline__ void run_schedule(const cpx<T>* __restrict__ coef,
                                              const uint2* __restrict__ meta, int len, int lane,
                                              const cpx<T>* __restrict__ pw,
@@ -383,6 +388,7 @@ __device__ __forceinline__ void run_schedule(const cpx<T>* __restrict__ coef,
   // running sums. A store happens for every record, to the entry when the
   // record is its last contribution, else to the lane's scratch slot, so the
   // loop has no data-dependent branch.
+  static_assert(F == 1 || F == 3, "one- and three-factor schedules");
   cpx<T> acc = czero<T>();
   for (int i0 = 0; i0 < len; i0 += 4) {
     uint2 m[4];
@@ -390,19 +396,30 @@ __device__ __forceinline__ void run_schedule(const cpx<T>* __restrict__ coef,
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int slot = (i0 + u) * kWarp + lane;
-      m[u] = meta[slot];
+      if constexpr (F == 1) {
+        m[u].x = reinterpret_cast<const unsigned*>(meta)[2 * slot];
+        m[u].y = 0u;
+      } else {
+        m[u] = meta[slot];
+      }
       c[u] = lds(&coef[slot]);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const unsigned lo = m[u].x, hi = m[u].y;
       p0[u] = lds(&pw[(lo >> 15) & 0x3ffu]);
-      p1[u] = lds(&pw[(lo >> 25) | ((hi & 7u) << 7)]);
-      p2[u] = lds(&pw[(hi >> 3) & 0x3ffu]);
+      if constexpr (F == 3) {
+        p1[u] = lds(&pw[(lo >> 25) | ((hi & 7u) << 7)]);
+        p2[u] = lds(&pw[(hi >> 3) & 0x3ffu]);
+      }
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const cpx<T> v = (c[u] * p0[u]) * (p1[u] * p2[u]);
+      cpx<T> v;
+      if constexpr (F == 1)
+        v = c[u] * p0[u];
+      else
+        v = (c[u] * p0[u]) * (p1[u] * p2[u]);
       const unsigned lo = m[u].x;
       const bool last = (lo >> 12) & kRecLast;
       acc = acc + v;
@@ -436,8 +453,12 @@ __device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, c
   cpx<T>* pw = ws_pw<T>(ws);
   power_table<T>(C, pw, ccast<T>(zl), lane);
   __syncwarp();
-  run_schedule<T>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws),
-                  reinterpret_cast<cpx<T>*>(ws.sink) + lane);
+  if (C.max_fac <= 1)
+    run_schedule<T, 1>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws),
+                       reinterpret_cast<cpx<T>*>(ws.sink) + lane);
+  else
+    run_schedule<T, 3>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws),
+                       reinterpret_cast<cpx<T>*>(ws.sink) + lane);
   __syncwarp();
 
   const cpx<T> gamma = ccast<T>(C.gamma);
@@ -509,6 +530,8 @@ __device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, c
 // multiplies its right-hand side by the reciprocal of its own pivot, and
 // piv[k] is the lane that then holds row k of X. Returns false for an
 // exactly zero pivot column (err_singular_matrix of lu_factor).
+constexpr int kGjGroup = 4;  // columns per uniform branch of the row update (NM > 8)
+
 template <int NM, int R, typename T>
 __device__ __forceinline__ bool gauss_jordan(cpx<T> (&a)[NM], cpx<T> (&r)[R], int N, int lane,
                                              int* piv) {
@@ -540,12 +563,24 @@ __device__ __forceinline__ bool gauss_jordan(cpx<T> (&a)[NM], cpx<T> (&r)[R], in
     const cpx<T> rp = shfl(rinv, p);
     // multiplier; the pivot row only shifts (l = 0)
     const cpx<T> l = isp ? czero<T>() : m0 * rp;
-    // next pivot column first, so that the next reduction can start early
-    a[0] = cfms(a[1], l, shfl(a[1], p));
-    m0 = a[0];
+    // Columns N-1-k and beyond are zero after this step; the update runs
+    // over groups of kGjGroup columns and skips (uniform branch) the
+    // groups that hold only zeros before and after it.
+    const int live = N - 1 - k;  // last column that is nonzero before the step
+    constexpr int G = (NM <= 8) ? NM : kGjGroup;  // narrow rows: one group
+    StaticFor<0, (NM + G - 1) / G>::run([&](auto gc) {
+      constexpr int g = decltype(gc)::value;
+      if (g == 0 || G * g <= live) {
 #pragma unroll
-    for (int j = 1; j + 1 < NM; ++j) a[j] = cfms(a[j + 1], l, shfl(a[j + 1], p));
-    a[NM - 1] = czero<T>();
+        for (int j = G * g; j < G * (g + 1) && j < NM; ++j) {
+          if (j + 1 < NM)
+            a[j] = cfms(a[j + 1], l, shfl(a[j + 1], p));
+          else
+            a[j] = czero<T>();
+        }
+      }
+    });
+    m0 = a[0];
 #pragma unroll
     for (int q = 0; q < R; ++q) r[q] = cfms(r[q], l, shfl(r[q], p));
   }

@@ -65,7 +65,8 @@ struct alignas(16) PlanHeader {
   int32_t n_levels;
   int32_t level_off[kMaxLevels + 1];  // word ranges per level (2 words per entry)
   int32_t pw_total;     // pw_size + n_pre: entries of the per-warp table
-  int32_t pad0_[2];
+  int32_t max_fac;      // most power-table factors of any Jacobian record (0..3)
+  int32_t pad0_;
   int32_t cnt_f[kWarp]; // records of each lane
   int32_t cnt_j[kWarp];
   int32_t deg[kMaxN];

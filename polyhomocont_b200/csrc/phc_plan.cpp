@@ -224,8 +224,13 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   }
   PreTable pre;
   pre.base = pw_size;
+  int max_fac = 0;
   for (auto& ent : jent)
-    for (auto& c : ent) pre.reduce(c.fac);
+    for (auto& c : ent) {
+      pre.reduce(c.fac);
+      max_fac = std::max(max_fac, (int)c.fac.size());
+    }
+  H.max_fac = max_fac;
   const int n_pre = (int)pre.entries.size();
   int n_levels = 0;
   for (int l : pre.level) n_levels = std::max(n_levels, l + 1);
