@@ -116,9 +116,12 @@ typedef struct {
   int32_t precision;       /* PHC_PREC_*                               */
   int32_t schedule;        /* PHC_SCHED_*                              */
   int32_t device;          /* CUDA device ordinal                      */
-  int32_t warps_per_block; /* 0 = autotuned                            */
+  int32_t warps_per_block; /* 0 = the value phc_autotune chose for this
+                              device, precision, schedule and row width,
+                              else 4                                    */
   int32_t blocks_per_sm;   /* persistent grid: 0 = max resident        */
-  int32_t chunk;           /* persistent refill granularity (paths), 0 = 1 */
+  int32_t chunk;           /* persistent refill granularity (paths), 0 = the
+                              tuned value, else 1                        */
   int32_t fp64_sticky;     /* mixed: FP64 steps after an FP32 failure, -1 = default */
   int32_t pad_;
 } phc_gpu_options;
@@ -283,6 +286,29 @@ int32_t phc_plan_destroy(phc_plan* plan);
 int32_t phc_plan_config(const phc_plan* plan, int32_t* warps_per_block,
                         int32_t* grid, int32_t* smem_bytes, int32_t* unknowns_cap,
                         int32_t* table_bytes);
+
+/* ---- autotuner -------------------------------------------------------- */
+/* Picks the launch configuration -- schedule (persistent refill or one path
+ * per warp), warps per block and refill chunk -- by timing the tracker on
+ * the first sample_paths paths of sys (0 = four paths per resident warp of
+ * the device) for each candidate, on gpu->device in gpu->precision. Writes
+ * the fastest into gpu->schedule, warps_per_block and chunk, and remembers
+ * it for this process: later plans and solves on the same device with the
+ * same precision, schedule and row width that pass warps_per_block = 0 or
+ * chunk = 0 get the tuned values. Allocates its own device buffers for the
+ * sample. The reference has no counterpart (its tracker is serial). */
+#define PHC_TUNE_MAX 32
+typedef struct {
+  int32_t ncand;                       /* candidates timed                 */
+  int32_t best;                        /* index of the chosen candidate    */
+  int32_t schedule[PHC_TUNE_MAX];
+  int32_t warps_per_block[PHC_TUNE_MAX];
+  int32_t chunk[PHC_TUNE_MAX];
+  double ms[PHC_TUNE_MAX];             /* best of the timed launches       */
+  int64_t sample_paths;
+} phc_tune_report;
+int32_t phc_autotune(const phc_system* sys, const phc_solve_options* opts,
+                     phc_gpu_options* gpu, int64_t sample_paths, phc_tune_report* report);
 
 /* ---- serving loop: continuous batching of whole systems ---------------- */
 typedef struct phc_server phc_server;

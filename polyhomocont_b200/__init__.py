@@ -273,6 +273,33 @@ def solve_paths(sys, options=None, gpu=None, k0=1, count=None, seed=None):
     return paths[:count], z[:count], x[:count], st
 
 
+def autotune(sys, options=None, gpu=None, sample_paths=0):
+    """Chooses the launch configuration (schedule, warps per block, refill
+    chunk) by timing the tracker on a sample of the system's paths
+    (phc_autotune). Returns (gpu_options, report): the options carry the
+    winner, and the report lists every candidate with its time in ms. The
+    choice is also remembered for this process: later plans and solves
+    that leave warps_per_block or chunk at 0 on the same device, precision,
+    schedule and row width use it."""
+    L = _abi.lib()
+    t, st = sys.table()
+    if st != PHC_OK:
+        raise PhcError(st, "table")
+    o = options if options is not None else default_options()
+    g = gpu if gpu is not None else default_gpu_options()
+    g2 = _abi.GpuOptions()
+    ctypes.memmove(ctypes.byref(g2), ctypes.byref(g), ctypes.sizeof(g))
+    rep = _abi.TuneReport()
+    st = L.phc_autotune(ctypes.byref(t), ctypes.byref(o), ctypes.byref(g2), int(sample_paths),
+                        ctypes.byref(rep))
+    _check_device_status(st, "phc_autotune")
+    if st != PHC_OK:
+        raise PhcError(st, "phc_autotune")
+    cands = [{"schedule": rep.schedule[i], "warps_per_block": rep.warps_per_block[i],
+              "chunk": rep.chunk[i], "ms": rep.ms[i]} for i in range(rep.ncand)]
+    return g2, {"candidates": cands, "best": rep.best, "sample_paths": rep.sample_paths}
+
+
 class Plan:
     """Device-resident plan: the compiled table lives in device memory and
     launches write device buffers (phc_plan_create / phc_plan_launch)."""

@@ -90,6 +90,15 @@ class ServerConfig(ctypes.Structure):
                 ("max_batch_paths", c_i32), ("mem_budget_bytes", c_i64), ("gpu", GpuOptions)]
 
 
+PHC_TUNE_MAX = 32
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [("ncand", c_i32), ("best", c_i32), ("schedule", c_i32 * PHC_TUNE_MAX),
+                ("warps_per_block", c_i32 * PHC_TUNE_MAX), ("chunk", c_i32 * PHC_TUNE_MAX),
+                ("ms", c_dbl * PHC_TUNE_MAX), ("sample_paths", c_i64)]
+
+
 # phc_path_out
 PATH_DTYPE = np.dtype([
     ("status", "<i4"), ("winding_number", "<i4"), ("endgame_status", "<i4"),
@@ -134,6 +143,8 @@ SIGNATURES = [
     ("phc_plan_launch_count", c_i32, [c_vp]),
     ("phc_plan_destroy", c_i32, [c_vp]),
     ("phc_plan_config", c_i32, [c_vp, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32)]),
+    ("phc_autotune", c_i32, [P(SystemC), P(SolveOptions), P(GpuOptions), c_i64,
+                             P(TuneReport)]),
     ("phc_server_create", c_i32, [P(ServerConfig), P(c_vp)]),
     ("phc_server_submit", c_i32, [c_vp, P(SystemC), P(SolveOptions), P(c_u64)]),
     ("phc_server_poll", c_i32, [c_vp, c_u64, P(c_i32)]),

@@ -205,11 +205,13 @@ int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, Lau
   }
   cfg->precision = (g.precision == PHC_PREC_MIXED) ? PHC_PREC_MIXED : PHC_PREC_FP64;
   cfg->persistent = (g.schedule == PHC_SCHED_PERSISTENT) ? 1 : 0;
-  cfg->chunk = g.chunk > 0 ? g.chunk : 1;
+  int tw = 4, tc = 1;
+  tuned_launch(device, cfg->precision, cfg->persistent, cfg->nm, &tw, &tc);
+  cfg->chunk = g.chunk > 0 ? g.chunk : tc;
   cfg->ws_bytes = ws_layout(hp.n, hp.S, hp.pw_size, cfg->precision == PHC_PREC_MIXED).bytes;
   const int plan_bytes = align16((int)hp.bytes.size());
   const int smax = device_smem_optin(device);
-  int warps = g.warps_per_block > 0 ? g.warps_per_block : 4;
+  int warps = g.warps_per_block > 0 ? g.warps_per_block : tw;
   warps = std::min(std::max(warps, 1), 8);
   while (warps > 1 && plan_bytes + warps * cfg->ws_bytes > smax) --warps;
   if (plan_bytes + warps * cfg->ws_bytes > smax) {

@@ -54,6 +54,9 @@ struct LaunchCfg {
 // Opt-in shared memory per block and SM count of a device (cached).
 int device_smem_optin(int device);
 int device_sms(int device);
+// Tuned launch parameters remembered by phc_autotune for a device,
+// precision, schedule and register-row width; false if none.
+bool tuned_launch(int device, int precision, int schedule, int nm, int* warps, int* chunk);
 // Resolves the launch configuration for a plan on a device.
 int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, LaunchCfg* cfg);
 // Launches the tracking kernel (phc_kernels.cu).
