@@ -186,6 +186,7 @@ class ClockSampler:
 # (profiles/track_kernel_n10_1024paths.md). The kernel is compute- and
 # latency-bound; its traffic is the table, the start data and the results.
 NCU_DRAM_BYTES_PER_LAUNCH = 158464
+SCHED_NAMES = {0: "grid", 1: "persistent"}
 
 
 def serving(P, W, nsys, device, load=0.7):
@@ -286,10 +287,11 @@ def main():
     hexps = np.ctypeslib.as_array(t.hexps, shape=(T * (n + 1),)).reshape(T, n + 1).copy()
     model = flops.unit_model(n, sysP.degrees(), hexps)
 
-    g_mixed = P.default_gpu_options(P.PHC_PREC_MIXED, P.PHC_SCHED_PERSISTENT, device=local)
-    # the all-FP64 tracker with the same persistent schedule: only the
-    # precision differs between the two arms
-    g_fp64 = P.default_gpu_options(P.PHC_PREC_FP64, P.PHC_SCHED_PERSISTENT, device=local)
+    # both arms get their launch configuration from the autotuner (timed on
+    # a sample of this system's paths, before and outside the timed region);
+    # the two arms then differ only in precision and in what the tuner chose
+    g_mixed, tune_m = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_MIXED, device=local))
+    g_fp64, tune_d = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_FP64, device=local))
     plan_m = P.Plan(sysP, gpu=g_mixed)
     plan_d = P.Plan(sysP, gpu=g_fp64)
     out_m = torch.zeros(npaths * 96, dtype=torch.uint8, device=dev)
@@ -408,10 +410,16 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (complex)",
             "data": "synthetic (seeded reference generator)",
             "config": {"workload": WORKLOAD, "paths": npaths, "precision": "mixed",
-                       "schedule": "persistent", "warps_per_block": cfg["warps_per_block"],
-                       "grid": cfg["grid"], "l2": "flushed between timed steps (256 MiB write)",
+                       "schedule": SCHED_NAMES[g_mixed.schedule],
+                       "warps_per_block": cfg["warps_per_block"], "chunk": g_mixed.chunk,
+                       "grid": cfg["grid"], "tuned_by": "phc_autotune on "
+                       f"{tune_m['sample_paths']} paths, {len(tune_m['candidates'])} candidates",
+                       "l2": "flushed between timed steps (256 MiB write)",
                        "parallelism": f"dp{world} (one system instance per GPU)"},
             "fp64_plain": {"value": v_fp64, "unit": "paths/s",
+                           "schedule": SCHED_NAMES[g_fp64.schedule],
+                           "warps_per_block": plan_d.config()["warps_per_block"],
+                           "chunk": g_fp64.chunk,
                            "ms_per_step": 1e3 * t_fp64_max / args.steps,
                            "achieved_tflops": fp64_achieved,
                            "frac_of_fp64_peak": fp64_achieved / peak64},
