@@ -539,13 +539,16 @@ __device__ __forceinline__ bool gauss_jordan(cpx<T> (&a)[NM], cpx<T> (&r)[R], in
   int mystep = -1;
   cpx<T> myrinv = czero<T>();
   cpx<T> m0 = a[0];
+  // The pivot search and the speculative reciprocal of step k+1 need only
+  // column 0 after step k, so they are issued as soon as that column is
+  // updated and run while the rest of step k's row update (shuffle-bound)
+  // is issued.
+  T d2 = m0.re * m0.re + m0.im * m0.im;
+  unsigned kmax;
+  int p = pivot_lane(d2, lane < N, lane, kmax);
+  T rd = rcp_nr(d2);
   for (int k = 0; k < N; ++k) {
     const bool cand = lane < N && !done;
-    const T d2 = m0.re * m0.re + m0.im * m0.im;
-    unsigned kmax;
-    int p = pivot_lane(d2, cand, lane, kmax);
-    // speculative reciprocal, used by the pivot lane only
-    const T rd = rcp_nr(d2);
     cpx<T> rinv = mkc<T>(m0.re * rd, -m0.im * rd);
     if (kmax == 0u) {
       // zero or tiny squares: decide with the modulus itself
@@ -563,16 +566,22 @@ __device__ __forceinline__ bool gauss_jordan(cpx<T> (&a)[NM], cpx<T> (&r)[R], in
     const cpx<T> rp = shfl(rinv, p);
     // multiplier; the pivot row only shifts (l = 0)
     const cpx<T> l = isp ? czero<T>() : m0 * rp;
-    // Columns N-1-k and beyond are zero after this step; the update runs
-    // over groups of kGjGroup columns and skips (uniform branch) the
-    // groups that hold only zeros before and after it.
+    // next pivot column, then the next step's search
+    a[0] = (NM > 1) ? cfms(a[1], l, shfl(a[1], p)) : czero<T>();
+    m0 = a[0];
+    d2 = m0.re * m0.re + m0.im * m0.im;
+    const int pn = pivot_lane(d2, lane < N && !done, lane, kmax);
+    rd = rcp_nr(d2);
+    // Columns N-1-k and beyond are zero after this step; the rest of the
+    // update runs over groups of kGjGroup columns and skips (uniform
+    // branch) the groups that hold only zeros before and after it.
     const int live = N - 1 - k;  // last column that is nonzero before the step
     constexpr int G = (NM <= 8) ? NM : kGjGroup;  // narrow rows: one group
     StaticFor<0, (NM + G - 1) / G>::run([&](auto gc) {
       constexpr int g = decltype(gc)::value;
       if (g == 0 || G * g <= live) {
 #pragma unroll
-        for (int j = G * g; j < G * (g + 1) && j < NM; ++j) {
+        for (int j = (G * g > 1 ? G * g : 1); j < G * (g + 1) && j < NM; ++j) {
           if (j + 1 < NM)
             a[j] = cfms(a[j + 1], l, shfl(a[j + 1], p));
           else
@@ -580,9 +589,9 @@ __device__ __forceinline__ bool gauss_jordan(cpx<T> (&a)[NM], cpx<T> (&r)[R], in
         }
       }
     });
-    m0 = a[0];
 #pragma unroll
     for (int q = 0; q < R; ++q) r[q] = cfms(r[q], l, shfl(r[q], p));
+    p = pn;
   }
 #pragma unroll
   for (int q = 0; q < R; ++q) r[q] = r[q] * myrinv;
