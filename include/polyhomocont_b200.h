@@ -287,6 +287,19 @@ int32_t phc_plan_config(const phc_plan* plan, int32_t* warps_per_block,
                         int32_t* grid, int32_t* smem_bytes, int32_t* unknowns_cap,
                         int32_t* table_bytes);
 
+/* ---- CUDA graphs of plan launches ------------------------------------- */
+/* Captures what phc_plan_launch(plan, k0, count, d_out, d_z, stream) issues
+ * -- the reset of the persistent queue and the tracker kernel -- into a
+ * CUDA graph and instantiates it; phc_graph_launch replays it on a stream
+ * with one call. The plan and the device buffers must outlive the graph.
+ * For a batch of paths that is solved repeatedly, or as a piece of a
+ * larger application graph. The reference has no counterpart. */
+typedef struct phc_graph phc_graph;
+int32_t phc_graph_create(phc_plan* plan, int64_t k0, int64_t count, phc_path_out* d_out,
+                         double* d_z, phc_graph** graph);
+int32_t phc_graph_launch(phc_graph* graph, void* stream);
+int32_t phc_graph_destroy(phc_graph* graph);
+
 /* ---- autotuner -------------------------------------------------------- */
 /* Picks the launch configuration -- schedule (persistent refill or one path
  * per warp), warps per block and refill chunk -- by timing the tracker on

@@ -273,6 +273,29 @@ def solve_paths(sys, options=None, gpu=None, k0=1, count=None, seed=None):
     return paths[:count], z[:count], x[:count], st
 
 
+class Graph:
+    """An instantiated CUDA graph of one plan launch (phc_graph_*)."""
+
+    def __init__(self, L, h):
+        self._L, self.h = L, h
+
+    def launch(self, stream=0):
+        st = self._L.phc_graph_launch(self.h, ctypes.c_void_p(stream))
+        if st != PHC_OK:
+            raise PhcError(st, "phc_graph_launch")
+
+    def close(self):
+        if self.h:
+            self._L.phc_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def autotune(sys, options=None, gpu=None, sample_paths=0):
     """Chooses the launch configuration (schedule, warps per block, refill
     chunk) by timing the tracker on a sample of the system's paths
@@ -326,6 +349,16 @@ class Plan:
                                      ctypes.c_void_p(d_z), ctypes.c_void_p(stream))
         if st != PHC_OK:
             raise PhcError(st, "phc_plan_launch")
+
+    def graph(self, k0, count, d_out, d_z):
+        """CUDA graph of launch(k0, count, d_out, d_z) (phc_graph_create);
+        replay it with Graph.launch(stream)."""
+        h = ctypes.c_void_p()
+        st = self._L.phc_graph_create(self.h, int(k0), int(count), ctypes.c_void_p(d_out),
+                                      ctypes.c_void_p(d_z), ctypes.byref(h))
+        if st != PHC_OK:
+            raise PhcError(st, "phc_graph_create")
+        return Graph(self._L, h)
 
     def config(self):
         w, g, s, nm, tb = (ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(),

@@ -143,6 +143,9 @@ SIGNATURES = [
     ("phc_plan_launch_count", c_i32, [c_vp]),
     ("phc_plan_destroy", c_i32, [c_vp]),
     ("phc_plan_config", c_i32, [c_vp, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32)]),
+    ("phc_graph_create", c_i32, [c_vp, c_i64, c_i64, c_vp, c_vp, P(c_vp)]),
+    ("phc_graph_launch", c_i32, [c_vp, c_vp]),
+    ("phc_graph_destroy", c_i32, [c_vp]),
     ("phc_autotune", c_i32, [P(SystemC), P(SolveOptions), P(GpuOptions), c_i64,
                              P(TuneReport)]),
     ("phc_server_create", c_i32, [P(ServerConfig), P(c_vp)]),

@@ -732,6 +732,65 @@ int32_t phc_plan_launch(phc_plan* p, int64_t k0, int64_t count, phc_path_out* d_
 
 int32_t phc_plan_launch_count(const phc_plan* p) { return p ? 1 : 0; }
 
+}  // extern "C"
+
+struct phc_graph {
+  int device = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" {
+
+int32_t phc_graph_create(phc_plan* p, int64_t k0, int64_t count, phc_path_out* d_out,
+                         double* d_z, phc_graph** out) {
+  if (!p || !out) return PHC_ERR_BAD_HANDLE;
+  *out = nullptr;
+  if (count <= 0 || k0 < 1 || k0 + count - 1 > p->hp.nstart || !d_out || !d_z)
+    return PHC_ERR_INVALID_INPUT;
+  PHC_CUDA(cudaSetDevice(p->device));
+  std::unique_ptr<phc_graph> g(new (std::nothrow) phc_graph());
+  if (!g) return PHC_ERR_OOM;
+  g->device = p->device;
+  cudaStream_t s = nullptr;
+  PHC_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  int st = PHC_OK;
+  if (e == cudaSuccess) {
+    st = phc_plan_launch(p, k0, count, d_out, d_z, s);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+    if (st == PHC_OK && e2 != cudaSuccess) e = e2;
+    g->graph = graph;
+  }
+  if (e == cudaSuccess && st == PHC_OK)
+    e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  cudaStreamDestroy(s);
+  if (st != PHC_OK || e != cudaSuccess) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    return st != PHC_OK ? st : cuda_fail(e, "graph capture");
+  }
+  *out = g.release();
+  return PHC_OK;
+}
+
+int32_t phc_graph_launch(phc_graph* g, void* stream) {
+  if (!g) return PHC_ERR_BAD_HANDLE;
+  PHC_CUDA(cudaSetDevice(g->device));
+  PHC_CUDA(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+  return PHC_OK;
+}
+
+int32_t phc_graph_destroy(phc_graph* g) {
+  if (!g) return PHC_ERR_BAD_HANDLE;
+  cudaSetDevice(g->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return PHC_OK;
+}
+
 int32_t phc_plan_config(const phc_plan* p, int32_t* warps, int32_t* grid, int32_t* smem,
                         int32_t* nm, int32_t* table_bytes) {
   if (!p) return PHC_ERR_BAD_HANDLE;
