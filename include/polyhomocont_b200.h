@@ -323,6 +323,24 @@ typedef struct {
 int32_t phc_autotune(const phc_system* sys, const phc_solve_options* opts,
                      phc_gpu_options* gpu, int64_t sample_paths, phc_tune_report* report);
 
+/* ---- compact request format (serving ingest) ---------------------------- */
+/* A system and optional solve_options as one byte string: a 24-byte header
+ * ("PHCR", version 1, n, total terms, flags), the options if flagged, the
+ * term count of each equation, then per term its coefficient (two float64)
+ * and its nonzero affine exponents as uint16 (variable, exponent) pairs.
+ * The packed counterpart of sparse_system%add_equation's input
+ * (src/sparse.f90:83-141); the reference itself has no wire format. */
+int64_t phc_request_size(const phc_system* sys, int32_t with_options);
+/* opts may be NULL (the request then carries none); *len = bytes written,
+ * or the bytes needed when cap is too small */
+int32_t phc_request_encode(const phc_system* sys, const phc_solve_options* opts, void* buf,
+                           int64_t cap, int64_t* len);
+/* Fills a fresh builder through phc_sparse_add_equation (the reference's
+ * validation and degree rules) and *opts (defaults when the request has
+ * none). Malformed input returns PHC_ERR_INVALID_INPUT. */
+int32_t phc_request_decode(const void* buf, int64_t len, phc_sparse* builder,
+                           phc_solve_options* opts);
+
 /* ---- serving loop: continuous batching of whole systems ---------------- */
 typedef struct phc_server phc_server;
 typedef struct {
@@ -341,6 +359,9 @@ int32_t phc_server_submit(phc_server* srv, const phc_system* sys,
                           const phc_solve_options* opts, uint64_t* ticket);
 /* *done = 1 once the result is ready; returns PHC_ERR_BAD_HANDLE for an
  * unknown ticket */
+/* phc_server_submit for a request in the compact format */
+int32_t phc_server_submit_request(phc_server* srv, const void* buf, int64_t len,
+                                  uint64_t* ticket);
 int32_t phc_server_poll(phc_server* srv, uint64_t ticket, int32_t* done);
 /* blocks until done or timeout_ms passed (PHC_ERR_NOT_READY); < 0 waits */
 int32_t phc_server_wait(phc_server* srv, uint64_t ticket, int64_t timeout_ms);

@@ -127,6 +127,33 @@ class SparseSystem:
         return int(self._L.phc_bezout(ctypes.byref(t))) if st == 0 else 0
 
 
+def encode_request(sys, options=None):
+    """The system (and options, if given) in the compact request format of
+    the serving path (phc_request_encode) as bytes."""
+    L = _abi.lib()
+    t, st = sys.table()
+    if st != PHC_OK:
+        raise PhcError(st, "table")
+    optr = ctypes.byref(options) if options is not None else None
+    size = int(L.phc_request_size(ctypes.byref(t), 1 if options is not None else 0))
+    buf = ctypes.create_string_buffer(max(size, 1))
+    n = ctypes.c_int64()
+    st = L.phc_request_encode(ctypes.byref(t), optr, buf, size, ctypes.byref(n))
+    if st != PHC_OK:
+        raise PhcError(st, "phc_request_encode")
+    return buf.raw[:n.value]
+
+
+def decode_request(data):
+    """(SparseSystem, solve_options, status) from a compact request
+    (phc_request_decode); status != 0 for a malformed request."""
+    s = SparseSystem()
+    o = SolveOptions()
+    buf = ctypes.create_string_buffer(bytes(data), max(len(data), 1))
+    st = s._L.phc_request_decode(buf, len(data), s.h, ctypes.byref(o))
+    return s, o, st
+
+
 class SolveResult:
     """type(solve_result), src/solve.f90:121-150. Arrays are 0-based with
     solutions as rows; the path index fields keep the reference's 1-based
@@ -476,6 +503,18 @@ class Server:
         if st != PHC_OK:
             return None, st
         self.n_of[ticket.value] = sys.nvars()
+        return ticket.value, st
+
+    def submit_request(self, data, n):
+        """Submits a request in the compact format (phc_server_submit_request);
+        n is its number of unknowns (for sizing the result). Returns
+        (ticket, status)."""
+        buf = ctypes.create_string_buffer(bytes(data), max(len(data), 1))
+        ticket = ctypes.c_uint64()
+        st = self._L.phc_server_submit_request(self.h, buf, len(data), ctypes.byref(ticket))
+        if st != PHC_OK:
+            return None, st
+        self.n_of[ticket.value] = int(n)
         return ticket.value, st
 
     def poll(self, ticket):

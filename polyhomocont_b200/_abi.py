@@ -148,7 +148,11 @@ SIGNATURES = [
     ("phc_graph_destroy", c_i32, [c_vp]),
     ("phc_autotune", c_i32, [P(SystemC), P(SolveOptions), P(GpuOptions), c_i64,
                              P(TuneReport)]),
+    ("phc_request_size", c_i64, [P(SystemC), c_i32]),
+    ("phc_request_encode", c_i32, [P(SystemC), P(SolveOptions), c_vp, c_i64, P(c_i64)]),
+    ("phc_request_decode", c_i32, [c_vp, c_i64, c_vp, P(SolveOptions)]),
     ("phc_server_create", c_i32, [P(ServerConfig), P(c_vp)]),
+    ("phc_server_submit_request", c_i32, [c_vp, c_vp, c_i64, P(c_u64)]),
     ("phc_server_submit", c_i32, [c_vp, P(SystemC), P(SolveOptions), P(c_u64)]),
     ("phc_server_poll", c_i32, [c_vp, c_u64, P(c_i32)]),
     ("phc_server_wait", c_i32, [c_vp, c_u64, c_i64]),

@@ -77,3 +77,32 @@ def test_shutdown_with_requests_in_flight():
     for i in range(8):
         srv.submit(W.build(P.SparseSystem, *W.stream_system(100 + i)))
     srv.close()
+
+
+def test_compact_requests_give_the_same_results():
+    """A request submitted in the compact wire format is solved exactly
+    like the same system submitted as a table."""
+    systems = [W.build(P.SparseSystem, *W.stream_system(200 + i)) for i in range(6)]
+    srv = P.Server(nslots=2)
+    try:
+        pairs = []
+        for s in systems:
+            t1, st1 = srv.submit(s)
+            t2, st2 = srv.submit_request(P.encode_request(s, P.default_options()), s.nvars())
+            assert st1 == 0 and st2 == 0
+            pairs.append((t1, t2))
+        for t1, t2 in pairs:
+            assert srv.wait(t1, 120000) == 0 and srv.wait(t2, 120000) == 0
+            r1, s1, _ = srv.result(t1)
+            r2, s2, _ = srv.result(t2)
+            assert s1 == s2 == 0
+            assert r1.nsolutions == r2.nsolutions and r1.ninfinite == r2.ninfinite
+            for key in ("status", "winding_number", "at_infinity", "singular", "is_real",
+                        "solution_index"):
+                assert np.array_equal(r1.paths[key], r2.paths[key]), key
+            assert np.array_equal(r1.x, r2.x)
+        bad = b"PHCR" + bytes(20)
+        t, st = srv.submit_request(bad, 1)
+        assert t is None and st == P.ERR_INVALID_INPUT
+    finally:
+        srv.close()
