@@ -86,6 +86,12 @@ __device__ __forceinline__ cpx<T> cfms(cpx<T> a, cpx<T> l, cpx<T> b) {
   return mkc<T>(fma_(-l.re, b.re, fma_(l.im, b.im, a.re)),
                 fma_(-l.re, b.im, fma_(-l.im, b.re, a.im)));
 }
+// acc + x*y as four fused multiply-adds
+template <typename T>
+__device__ __forceinline__ cpx<T> cfma(cpx<T> acc, cpx<T> x, cpx<T> y) {
+  return mkc<T>(fma_(x.re, y.re, fma_(-x.im, y.im, acc.re)),
+                fma_(x.re, y.im, fma_(x.im, y.re, acc.im)));
+}
 // Complex division by Smith's method (R. L. Smith, CACM 5 (1962) 435),
 // the range-reducing division of Fortran compilers.
 template <typename T>
@@ -381,13 +387,12 @@ template <typename T, int F>
 __device__ __forceinline__ void run_schedule(const cpx<T>* __restrict__ coef,
                                              const uint2* __restrict__ meta, int len, int lane,
                                              const cpx<T>* __restrict__ pw,
-                                             cpx<T>* __restrict__ out, cpx<T>* __restrict__ sink) {
+                                             cpx<T>* __restrict__ out) {
   // All lanes run len (the longest lane's count, a multiple of 4: shorter
   // lanes read zero padding records). Records are processed four at a time:
   // the loads of a batch are issued together, then the products, then the
-  // running sums. A store happens for every record, to the entry when the
-  // record is its last contribution, else to the lane's scratch slot, so the
-  // loop has no data-dependent branch.
+  // running sums. The sum is stored (a predicated store, not a branch) when
+  // the record is the entry's last contribution.
   static_assert(F == 1 || F == 3, "one- and three-factor schedules");
   cpx<T> acc = czero<T>();
   for (int i0 = 0; i0 < len; i0 += 4) {
@@ -423,7 +428,7 @@ __device__ __forceinline__ void run_schedule(const cpx<T>* __restrict__ coef,
       const unsigned lo = m[u].x;
       const bool last = (lo >> 12) & kRecLast;
       acc = acc + v;
-      sts(last ? &out[lo & 0x3ffu] : sink, acc);
+      if (last) sts(&out[lo & 0x3ffu], acc);
       acc = last ? czero<T>() : acc;
     }
   }
@@ -454,11 +459,9 @@ __device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, c
   power_table<T>(C, pw, ccast<T>(zl), lane);
   __syncwarp();
   if (C.max_fac <= 1)
-    run_schedule<T, 1>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws),
-                       reinterpret_cast<cpx<T>*>(ws.sink) + lane);
+    run_schedule<T, 1>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws));
   else
-    run_schedule<T, 3>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws),
-                       reinterpret_cast<cpx<T>*>(ws.sink) + lane);
+    run_schedule<T, 3>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws));
   __syncwarp();
 
   const cpx<T> gamma = ccast<T>(C.gamma);
@@ -473,16 +476,19 @@ __device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, c
   const bool eq = lane < n;
   const int row = lane < n ? lane : n;
   const cpx<T>* Jr = ws_j<T>(ws) + row * S;
+  // row scale: (1 - t) for an equation row, 1 for the patch row, 0 for the
+  // lanes beyond it (their rows are all zero)
+  const cpx<T> sc = eq ? omt : (lane == n ? cone<T>() : czero<T>());
   cpx<T> f0 = czero<T>(), f1 = czero<T>();
 #pragma unroll
   for (int j = 0; j < NM; ++j) {
     if (j < N) {
       const cpx<T> jij = lds(&Jr[j]);
       if (j & 1)
-        f1 = f1 + jij * lds(&zrow[j]);
+        f1 = cfma(f1, jij, lds(&zrow[j]));
       else
-        f0 = f0 + jij * lds(&zrow[j]);
-      a[j] = eq ? omt * jij : jij;
+        f0 = cfma(f0, jij, lds(&zrow[j]));
+      a[j] = sc * jij;
     } else {
       a[j] = czero<T>();
     }
@@ -499,18 +505,14 @@ __device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, c
   const T dd = (T)C.deg;
   const cpx<T> dg = eq ? (dd * gt) * zd1 : czero<T>();
   const cpx<T> dw = eq ? (dd * (gt * bi)) * wd1 : czero<T>();
+  // dg and dw are zero outside the equation rows
 #pragma unroll
   for (int j = 0; j < NM; ++j) {
     if (j == lane) a[j] = a[j] + dg;
     if (j == n) a[j] = a[j] - dw;
   }
-  cpx<T> hh = eq ? gt * g + omt * f : mkc<T>(f.re - T(1), f.im);
+  cpx<T> hh = eq ? gt * g + omt * f : (lane == n ? mkc<T>(f.re - T(1), f.im) : czero<T>());
   cpx<T> hht = eq ? gamma * g - f : czero<T>();
-  if (lane > n) {
-    hh = hht = czero<T>();
-#pragma unroll
-    for (int j = 0; j < NM; ++j) a[j] = czero<T>();
-  }
   h = ccast<double>(hh);
   ht = ccast<double>(hht);
 }
