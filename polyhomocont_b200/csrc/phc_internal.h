@@ -135,6 +135,10 @@ struct KParamsBatch {
   int32_t pad_;
   int64_t total_paths;
   unsigned long long* counter;
+  // finished paths per request, in host memory mapped into the device (may
+  // be null): the host finishes a request as soon as its count is complete,
+  // while the rest of the batch is still running
+  unsigned int* done;
 };
 
 // Cold per-path state of the tracker state machine, kept in shared memory

@@ -50,7 +50,8 @@ struct Request {
   Clock::time_point t_submit, t_done;
   bool done = false;
   // placement inside a batch
-  size_t off_plan = 0, off_out = 0, off_z = 0, off_x = 0;
+  size_t off_plan = 0, off_out = 0, off_z = 0, off_x = 0, end = 0;
+  int stage = 0;  // 0: paths running, 1: results being copied, 2: finished
   LaunchCfg cfg;
 
   phc_system view() const {
@@ -67,7 +68,12 @@ struct Request {
 
 struct Slot {
   cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
+  cudaStream_t copy = nullptr;  // per-request result copies
+  cudaEvent_t done = nullptr;   // the batch kernel has finished
+  unsigned int* done_h = nullptr;  // finished paths per request (mapped host memory)
+  unsigned int* done_d = nullptr;  // the same array as the device sees it
+  std::vector<cudaEvent_t> copied;  // per request of the batch
+  int nfinished = 0;
   void* dbuf = nullptr;
   size_t dcap = 0;
   unsigned char* hbuf = nullptr;  // pinned: plans in, results out
@@ -119,6 +125,8 @@ size_t layout_batch(std::vector<std::shared_ptr<Request>>& b) {
     off += up256((size_t)r->npaths * (r->n + 1) * 16);
     r->off_x = off;
     off += up256((size_t)r->npaths * r->n * 16);
+    r->end = off;
+    r->stage = 0;
   }
   return off;
 }
@@ -208,6 +216,10 @@ int launch_batch(phc_server* S, Slot& s) {
   kb.slice_bytes = slice;
   kb.total_paths = total;
   kb.counter = s.counters;
+  // the slot is free, so the previous batch's kernel has finished with it
+  std::memset(s.done_h, 0, s.batch.size() * sizeof(unsigned int));
+  kb.done = s.done_d;
+  s.nfinished = 0;
   const int64_t per = (int64_t)warps * kb.chunk;
   const int grid =
       (int)std::min<int64_t>((int64_t)device_sms(S->cfg.device) * bps, (total + per - 1) / per);
@@ -217,10 +229,8 @@ int launch_batch(phc_server* S, Slot& s) {
   if (e != cudaSuccess) return cuda_fail(e, "server counter reset");
   e = launch_track_batch(nm, prec, warps, smem, kb, grid, s.stream);
   if (e != cudaSuccess) return cuda_fail(e, "server kernel launch");
-  // results of the whole batch in one copy
-  e = cudaMemcpyAsync(s.hbuf + plan_end, dev + plan_end, bytes - plan_end,
-                      cudaMemcpyDeviceToHost, s.stream);
-  if (e != cudaSuccess) return cuda_fail(e, "server D2H");
+  // each request's results are copied back as soon as its paths are done
+  // (see engine_main); the event marks the end of the whole batch
   e = cudaEventRecord(s.done, s.stream);
   if (e != cudaSuccess) return cuda_fail(e, "server event");
   return PHC_OK;
@@ -257,22 +267,69 @@ void engine_main(phc_server* S) {
   std::unique_lock<std::mutex> lk(S->mu);
   for (;;) {
     bool progressed = false;
-    // 1. completions
+    // 1. completions, request by request: a request whose paths are all
+    // counted (or whose batch kernel has ended) gets its results copied back
+    // on the slot's copy stream while the rest of the batch keeps running;
+    // once the copy has landed it is finished on the host
     for (auto& s : S->slots) {
       if (!s.busy) continue;
-      if (cudaEventQuery(s.done) != cudaSuccess) continue;
-      const auto now = Clock::now();
-      for (auto& r : s.batch) {
-        finish_request(*r, s.hbuf);
-        r->t_done = now;
-        r->done = true;
-        S->completed++;
+      const cudaError_t kq = cudaEventQuery(s.done);
+      const bool kfin = (kq == cudaSuccess);
+      if (kq != cudaSuccess && kq != cudaErrorNotReady) {
+        // the batch kernel failed: its unfinished requests fail with it
+        set_last_error(cudaGetErrorString(kq));
+        for (auto& r : s.batch) {
+          if (r->stage == 2) continue;
+          r->status = PHC_ERR_CUDA;
+          r->t_done = Clock::now();
+          r->done = true;
+          r->stage = 2;
+          S->completed++;
+          s.nfinished++;
+        }
       }
-      S->mem_in_use -= s.bytes;
-      s.batch.clear();
-      s.busy = false;
-      progressed = true;
-      S->cv.notify_all();
+      unsigned char* dev = static_cast<unsigned char*>(s.dbuf);
+      for (size_t i = 0; i < s.batch.size(); ++i) {
+        Request& r = *s.batch[i];
+        if (r.stage == 0) {
+          const unsigned int cnt = reinterpret_cast<volatile unsigned int*>(s.done_h)[i];
+          if (kfin || cnt >= (unsigned int)r.npaths) {
+            cudaError_t e = cudaMemcpyAsync(s.hbuf + r.off_out, dev + r.off_out,
+                                            r.end - r.off_out, cudaMemcpyDeviceToHost, s.copy);
+            if (e == cudaSuccess) e = cudaEventRecord(s.copied[i], s.copy);
+            if (e != cudaSuccess) {
+              cuda_fail(e, "server D2H");
+              r.status = PHC_ERR_CUDA;
+              r.t_done = Clock::now();
+              r.done = true;
+              r.stage = 2;
+              S->completed++;
+              s.nfinished++;
+              progressed = true;
+              continue;
+            }
+            r.stage = 1;
+            progressed = true;
+          }
+        }
+        if (r.stage == 1 && cudaEventQuery(s.copied[i]) == cudaSuccess) {
+          finish_request(r, s.hbuf);
+          r.t_done = Clock::now();
+          r.done = true;
+          r.stage = 2;
+          S->completed++;
+          s.nfinished++;
+          progressed = true;
+          S->cv.notify_all();
+        }
+      }
+      if ((kfin || (kq != cudaErrorNotReady)) && s.nfinished == (int)s.batch.size()) {
+        S->mem_in_use -= s.bytes;
+        s.batch.clear();
+        s.busy = false;
+        progressed = true;
+        S->cv.notify_all();
+      }
     }
     // 2. admissions: fill every free slot with pending requests (FIFO)
     for (auto& s : S->slots) {
@@ -359,6 +416,20 @@ int32_t phc_server_create(const phc_server_config* cfg, phc_server** out) {
     if (e != cudaSuccess) return cuda_fail(e, "server event");
     e = cudaMalloc((void**)&s.counters, sizeof(unsigned long long));
     if (e != cudaSuccess) return cuda_fail(e, "server counter");
+    e = cudaStreamCreateWithFlags(&s.copy, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "server copy stream");
+    const int max_sys = S->cfg.max_batch_systems > 0 ? S->cfg.max_batch_systems : 256;
+    e = cudaHostAlloc((void**)&s.done_h, (size_t)max_sys * sizeof(unsigned int),
+                      cudaHostAllocMapped);
+    if (e != cudaSuccess) return cuda_fail(e, "server path counters");
+    std::memset(s.done_h, 0, (size_t)max_sys * sizeof(unsigned int));
+    e = cudaHostGetDevicePointer((void**)&s.done_d, s.done_h, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "server path counters (device view)");
+    s.copied.assign(max_sys, nullptr);
+    for (auto& ev : s.copied) {
+      e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e != cudaSuccess) return cuda_fail(e, "server copy event");
+    }
     // initial buffers sized for a typical batch, grown on demand
     int st = grow(s, (size_t)1 << 22, S->retired_host);
     if (st != PHC_OK) return st;
@@ -509,6 +580,11 @@ int32_t phc_server_destroy(phc_server* S) {
     if (s.hbuf) cudaFreeHost(s.hbuf);
     if (s.counters) cudaFree(s.counters);
     if (s.done) cudaEventDestroy(s.done);
+    if (s.copy) cudaStreamSynchronize(s.copy);
+    for (auto ev : s.copied)
+      if (ev) cudaEventDestroy(ev);
+    if (s.done_h) cudaFreeHost(s.done_h);
+    if (s.copy) cudaStreamDestroy(s.copy);
     if (s.stream) cudaStreamDestroy(s.stream);
   }
   for (void* h : S->retired_host) cudaFreeHost(h);

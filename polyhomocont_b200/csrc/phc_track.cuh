@@ -1016,6 +1016,13 @@ __global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb)
     double* z = reinterpret_cast<double*>(kb.base + S.z_off) + 2 * kl * N;
     double* x = S.x_off >= 0 ? reinterpret_cast<double*>(kb.base + S.x_off) + 2 * kl * n : nullptr;
     track_one<NM, PREC>(P, C, ws, *stp, *opts, kl + 1, lane, out, z, x);
+    if (kb.done != nullptr) {
+      // every lane's result stores are made visible system-wide before the
+      // path is counted as finished
+      __threadfence_system();
+      __syncwarp();
+      if (lane == 0) atomicAdd_system(&kb.done[lo], 1u);
+    }
   }
 }
 
