@@ -40,28 +40,49 @@ def finish_solve(n, paths, x, options=None):
     return res
 
 
+class ShardFailure(RuntimeError):
+    """A rank could not track its path range; raised on every rank that
+    reaches the gather (rank 0 names the failed ranks)."""
+
+
 def solve_sharded(sys, rank, world, group=None, options=None, gpu=None, runner=None):
     """solve() over `world` ranks. runner(k0, count) -> (paths, z, x) tracks a
     path range; by default the GPU (phc_solve_paths on this rank's device).
-    Returns the SolveResult on rank 0 and None elsewhere."""
+    Returns the SolveResult on rank 0 and None elsewhere.
+
+    Failure handling: a rank whose tracking raises still takes part in the
+    gather, with an error record instead of its paths, so rank 0 learns at
+    once which ranks failed and raises ShardFailure, and the failed rank
+    re-raises its own error. A rank that dies outright leaves the gather to
+    the process group's timeout, which ends it with an error on the others."""
     import torch.distributed as dist
     from . import default_gpu_options, default_options, solve_paths
     o = options if options is not None else default_options()
     npaths = sys.bezout()
     n = sys.nvars()
     k0, count = path_range(npaths, rank, world)
-    if runner is None:
-        g = gpu if gpu is not None else default_gpu_options(device=rank)
-        paths, z, x, st = solve_paths(sys, o, g, k0=k0, count=count)
-        if st != 0:
-            raise RuntimeError(f"solve_paths on rank {rank}: status {st}")
-    else:
-        paths, z, x = runner(k0, count)
+    err = None
+    try:
+        if runner is None:
+            g = gpu if gpu is not None else default_gpu_options(device=rank)
+            paths, z, x, st = solve_paths(sys, o, g, k0=k0, count=count)
+            if st != 0:
+                raise RuntimeError(f"solve_paths on rank {rank}: status {st}")
+        else:
+            paths, z, x = runner(k0, count)
+        mine = (k0, np.asarray(paths), np.asarray(z), np.asarray(x))
+    except Exception as e:  # reported through the gather, re-raised below
+        err = e
+        mine = (k0, None, None, f"{type(e).__name__}: {e}")
     parts = [None] * world if rank == 0 else None
-    dist.gather_object((k0, np.asarray(paths), np.asarray(z), np.asarray(x)), parts,
-                       dst=0, group=group)
+    dist.gather_object(mine, parts, dst=0, group=group)
+    if err is not None:
+        raise ShardFailure(f"rank {rank} failed to track paths {k0}..{k0 + count - 1}") from err
     if rank != 0:
         return None
+    failed = [(r, p[3]) for r, p in enumerate(parts) if p[1] is None]
+    if failed:
+        raise ShardFailure("ranks failed: " + "; ".join(f"{r}: {m}" for r, m in failed))
     parts.sort(key=lambda p: p[0])
     paths = np.concatenate([p[1] for p in parts])
     z = np.concatenate([p[2] for p in parts])

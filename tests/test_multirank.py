@@ -85,3 +85,59 @@ def test_path_ranges_partition():
                 assert a + ca == b
             assert sum(c for _, c in ks) == npaths
             assert max(c for _, c in ks) - min(c for _, c in ks) <= 1
+
+
+def _worker_failing(rank, world, port, mode, outdir):
+    """Rank 1 fails; rank 0 must learn of it (an error, never a hang)."""
+    import time
+    import sys
+    from datetime import timedelta
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    from oracle import oracle as O
+    import polyhomocont_b200 as P
+    from polyhomocont_b200 import shard
+    from polyhomocont_b200 import workloads as W
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=5))
+    n, eqs = W.katsura(3)
+    so = W.build(O.SparseSystem, n, eqs)
+    sp = W.build(P.SparseSystem, n, eqs)
+
+    def runner(k0, count):
+        if rank == 1:
+            if mode == "exit":
+                os._exit(0)  # the rank dies without a word
+            raise RuntimeError("injected tracking failure")
+        p, z, x, st = O.solve_paths(so, k0=k0, count=count)
+        return p, z, x
+
+    t0 = time.time()
+    outcome = "returned"
+    try:
+        shard.solve_sharded(sp, rank, world, runner=runner)
+    except Exception as e:  # noqa: BLE001 - the outcome is the test's subject
+        outcome = f"{type(e).__name__}: {e}"
+    with open(os.path.join(outdir, f"rank{rank}.txt"), "w") as f:
+        f.write(f"{time.time() - t0:.3f}\n{outcome}\n")
+    try:
+        dist.destroy_process_group()
+    except Exception:  # noqa: BLE001 - the peer may be gone
+        pass
+
+
+@pytest.mark.parametrize("mode", ["raise", "exit"])
+def test_failed_rank_is_detected(tmp_path, mode):
+    from polyhomocont_b200 import build as B
+    B.build()
+    mp.start_processes(_worker_failing, args=(2, _free_port(), mode, str(tmp_path)), nprocs=2,
+                       join=True, start_method="spawn")
+    t0, out0 = open(os.path.join(tmp_path, "rank0.txt")).read().split("\n", 1)
+    assert float(t0) < 60.0
+    assert out0.startswith(("ShardFailure", "RuntimeError", "DistBackendError")), out0
+    if mode == "raise":
+        assert "ranks failed: 1" in out0 and "injected tracking failure" in out0
+        t1, out1 = open(os.path.join(tmp_path, "rank1.txt")).read().split("\n", 1)
+        assert out1.startswith("ShardFailure")
