@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serving-systems", type=int, default=4096,
                     help="systems in the serving stream (0 skips the serving leg)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="default launch configuration instead of the autotuner's "
+                         "(for profiling: the timed launches then follow the warm-up directly)")
     return ap.parse_args()
 
 
@@ -290,8 +293,15 @@ def main():
     # both arms get their launch configuration from the autotuner (timed on
     # a sample of this system's paths, before and outside the timed region);
     # the two arms then differ only in precision and in what the tuner chose
-    g_mixed, tune_m = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_MIXED, device=local))
-    g_fp64, tune_d = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_FP64, device=local))
+    if args.no_tune:
+        g_mixed = P.default_gpu_options(P.PHC_PREC_MIXED, device=local)
+        g_fp64 = P.default_gpu_options(P.PHC_PREC_FP64, device=local)
+        tune_m = {"sample_paths": 0, "candidates": []}
+    else:
+        g_mixed, tune_m = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_MIXED,
+                                                                     device=local))
+        g_fp64, tune_d = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_FP64,
+                                                                    device=local))
     plan_m = P.Plan(sysP, gpu=g_mixed)
     plan_d = P.Plan(sysP, gpu=g_fp64)
     out_m = torch.zeros(npaths * 96, dtype=torch.uint8, device=dev)
@@ -412,8 +422,10 @@ def main():
             "config": {"workload": WORKLOAD, "paths": npaths, "precision": "mixed",
                        "schedule": SCHED_NAMES[g_mixed.schedule],
                        "warps_per_block": cfg["warps_per_block"], "chunk": g_mixed.chunk,
-                       "grid": cfg["grid"], "tuned_by": "phc_autotune on "
-                       f"{tune_m['sample_paths']} paths, {len(tune_m['candidates'])} candidates",
+                       "grid": cfg["grid"],
+                       "tuned_by": ("defaults (--no-tune)" if args.no_tune else "phc_autotune on "
+                                    f"{tune_m['sample_paths']} paths, "
+                                    f"{len(tune_m['candidates'])} candidates"),
                        "l2": "flushed between timed steps (256 MiB write)",
                        "parallelism": f"dp{world} (one system instance per GPU)"},
             "fp64_plain": {"value": v_fp64, "unit": "paths/s",
