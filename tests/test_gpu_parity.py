@@ -156,3 +156,26 @@ def test_cfg2_parity_sample(orc):
             assert np.array_equal(pg[key], pr[key]), key
         d = np.max(np.abs(xg - xr), axis=1) / np.maximum(1.0, np.max(np.abs(xr), axis=1))
         assert d.max() <= TOL_REGULAR
+
+
+@pytest.mark.parametrize("n", [16, 20, 28])
+def test_wide_rows_parity_sample(orc, n):
+    """Random sparse quadratic systems whose N = n+1 unknowns need the wider
+    register rows (18, 24, 32 columns: the elimination without column-group
+    branches for 24 and 32, spilling kernels included); first 24 paths,
+    both precisions, against the restatement."""
+    n_, eqs = W.sparse_quadratic(n, 24, W.seed_for(5, 100 + n))
+    so = W.build(orc.SparseSystem, n_, eqs)
+    sp = W.build(P.SparseSystem, n_, eqs)
+    pr, zr, xr, st = orc.solve_paths(so, count=24, nthreads=8)
+    assert st == 0
+    for prec in (P.PHC_PREC_FP64, P.PHC_PREC_MIXED):
+        pg, zg, xg, st2 = P.solve_paths(sp, gpu=P.default_gpu_options(precision=prec), count=24)
+        assert st2 == 0
+        for key in ("status", "winding_number", "at_infinity", "singular", "is_real"):
+            assert np.array_equal(pg[key], pr[key]), (key, prec)
+        fin = (pr["status"] == 0) & (pr["at_infinity"] == 0)
+        if fin.any():
+            d = np.max(np.abs(xg[fin] - xr[fin]), axis=1) / np.maximum(
+                1.0, np.max(np.abs(xr[fin]), axis=1))
+            assert d.max() <= TOL_REGULAR, (d.max(), prec)
