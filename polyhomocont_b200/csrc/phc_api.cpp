@@ -342,23 +342,60 @@ static int run_paths_sync(const HostPlan& hp, const phc_solve_options& so,
 // ---------------------------------------------------------------------------
 // bookkeeping (src/solve.f90:193-213, :330-426)
 // ---------------------------------------------------------------------------
-static double norm_inf_c(const double* v, int n) {
+static double norm_inf_exact(const double* v, int n) {
   double r = 0.0;
   for (int i = 0; i < n; ++i) r = std::max(r, std::hypot(v[2 * i], v[2 * i + 1]));
   return r;
 }
 
+// Squared moduli decide a comparison with |.| (hypot) unless they are
+// within a relative kSqMargin of the threshold; only then is hypot itself
+// compared, so every decision is the one the hypot test makes. Squares of
+// magnitudes outside [kSqLo, kSqHi] could over- or underflow: those take
+// the exact path.
+constexpr double kSqMargin = 1e-12;
+constexpr double kSqLo = 1e-140, kSqHi = 1e140;
+
+// ||v||_inf (norm_inf, src/linalg.f90:176-189) with one hypot: the exact
+// maximum is among the components whose square is within the margin of
+// the largest square.
+static double norm_inf_c(const double* v, int n) {
+  double m2 = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double s = v[2 * i] * v[2 * i] + v[2 * i + 1] * v[2 * i + 1];
+    if (!(s <= kSqHi)) return norm_inf_exact(v, n);  // huge or NaN
+    m2 = std::max(m2, s);
+  }
+  if (m2 < kSqLo) return norm_inf_exact(v, n);
+  double r = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double s = v[2 * i] * v[2 * i] + v[2 * i + 1] * v[2 * i + 1];
+    if (s >= m2 * (1.0 - kSqMargin)) r = std::max(r, std::hypot(v[2 * i], v[2 * i + 1]));
+  }
+  return r;
+}
+
 // The reference's find (src/solve.f90:379-400) scans all stored points and
 // returns the first (lowest index) within tol * max(1, ||x||). PointSet
-// returns the same index without the O(P) scan: points are ordered by the
-// real part of their first coordinate, any match lies within the window
-// |Re x_1 - Re s_1| <= tol * max(1, ||x||), and the lowest index among the
-// matches in that window is the first match of the scan. Points or queries
-// with non-finite values take the linear scan, exactly as the reference.
+// returns the same index without the O(P) scan: any match lies within the
+// window |Re x_1 - Re s_1| <= tol * max(1, ||x||), so the points are
+// hashed by Re x_1 into buckets of width 64*tol, a query visits the
+// buckets its window covers, and the lowest index among the matches there
+// is the first match of the scan. Points or queries with non-finite values,
+// and windows wider than 64 buckets, take the linear scan, exactly as the
+// reference.
 class PointSet {
  public:
-  PointSet(int n, double tol) : n_(n), tol_(tol) {}
-  int size() const { return (int)(pts_.size() / (2 * (size_t)n_)); }
+  PointSet(int n, double tol, int64_t expect)
+      : n_(n), tol_(tol), width_(64.0 * tol) {
+    size_t cap = 64;
+    while (cap < 2 * (size_t)std::max<int64_t>(expect, 1)) cap <<= 1;
+    keys_.assign(cap, 0);
+    heads_.assign(cap, -1);
+    pts_.reserve((size_t)std::max<int64_t>(expect, 1) * 2 * n);
+    next_.reserve((size_t)std::max<int64_t>(expect, 1));
+  }
+  int size() const { return (int)next_.size(); }
   const std::vector<double>& data() const { return pts_; }
 
   int find(const double* x) const {
@@ -370,46 +407,104 @@ class PointSet {
       if (best >= 0 && j >= best) return;
       if (within(x, j, rho)) best = j;
     };
-    if (!std::isfinite(rho) || !std::isfinite(x0)) {
+    const double margin = 1e-12 * (std::fabs(x0) + rho) + 1e-300;
+    const double lo = x0 - rho - margin, hi = x0 + rho + margin;
+    if (!std::isfinite(rho) || !std::isfinite(x0) || !(width_ > 0.0) ||
+        (hi - lo) > 64.0 * width_ || std::fabs(x0) > 1e15 * width_) {
       for (int j = 0; j < size(); ++j) test(j);
-    } else {
-      const double margin = 1e-12 * (std::fabs(x0) + rho) + 1e-300;
-      auto lo = ordered_.lower_bound(x0 - rho - margin);
-      auto hi = ordered_.upper_bound(x0 + rho + margin);
-      for (auto it = lo; it != hi; ++it) test(it->second);
-      for (int j : special_) test(j);
+      return best < 0 ? 0 : best + 1;
     }
+    const long long b0 = bucket(lo), b1 = bucket(hi);
+    for (long long b = b0; b <= b1; ++b)
+      for (int j = head(b); j >= 0; j = next_[j]) test(j);
+    for (int j : special_) test(j);
     return best < 0 ? 0 : best + 1;
   }
 
   void add(const double* x) {
     const int j = size();
     pts_.insert(pts_.end(), x, x + 2 * (size_t)n_);
-    if (std::isfinite(x[0]))
-      ordered_.emplace(x[0], j);
-    else
+    if (std::isfinite(x[0]) && width_ > 0.0 && std::fabs(x[0]) <= 1e15 * width_) {
+      const long long b = bucket(x[0]);
+      size_t slot = probe(b);
+      if (heads_[slot] < 0) {
+        keys_[slot] = b;
+        ++used_;
+      }
+      next_.push_back(heads_[slot]);
+      heads_[slot] = j;
+      if (2 * used_ > keys_.size()) rehash();
+    } else {
+      next_.push_back(-1);
       special_.push_back(j);
+    }
   }
 
  private:
+  long long bucket(double v) const { return (long long)std::floor(v / width_); }
+  size_t hash(long long b) const {
+    return (size_t)(((unsigned long long)b * 0x9E3779B97F4A7C15ull) >> 17);
+  }
+  // slot of bucket b: its own, or the empty one where it would go
+  size_t probe(long long b) const {
+    const size_t mask = keys_.size() - 1;
+    size_t s = hash(b) & mask;
+    while (heads_[s] >= 0 && keys_[s] != b) s = (s + 1) & mask;
+    return s;
+  }
+  int head(long long b) const {
+    const size_t s = probe(b);
+    return heads_[s] >= 0 ? heads_[s] : -1;
+  }
+  void rehash() {
+    std::vector<long long> k2;
+    std::vector<int> h2;
+    k2.swap(keys_);
+    h2.swap(heads_);
+    keys_.assign(2 * k2.size(), 0);
+    heads_.assign(2 * k2.size(), -1);
+    for (size_t s = 0; s < k2.size(); ++s) {
+      if (h2[s] < 0) continue;
+      const size_t t = probe(k2[s]);
+      keys_[t] = k2[s];
+      heads_[t] = h2[s];
+    }
+  }
+  // max_i |x_i - p_i| <= rho, decided on squares away from the threshold
   bool within(const double* x, int j, double rho) const {
     const double* p = pts_.data() + (size_t)j * 2 * n_;
+    const double r2 = rho * rho;
+    bool exact = !(r2 >= kSqLo && r2 <= kSqHi);
+    double m2 = 0.0;
+    for (int i = 0; i < n_ && !exact; ++i) {
+      const double dr = x[2 * i] - p[2 * i], di = x[2 * i + 1] - p[2 * i + 1];
+      const double s = dr * dr + di * di;
+      if (!(s <= kSqHi)) exact = true;  // huge or NaN
+      m2 = std::max(m2, s);
+    }
+    if (!exact) {
+      if (m2 <= r2 * (1.0 - kSqMargin)) return true;
+      if (m2 >= r2 * (1.0 + kSqMargin)) return false;
+    }
     double d = 0.0;
     for (int i = 0; i < n_; ++i)
       d = std::max(d, std::hypot(x[2 * i] - p[2 * i], x[2 * i + 1] - p[2 * i + 1]));
     return d <= rho;
   }
   int n_;
-  double tol_;
+  double tol_, width_;
   std::vector<double> pts_;
-  std::multimap<double, int> ordered_;
+  std::vector<int> next_;         // previous point in the same bucket, or -1
+  std::vector<long long> keys_;   // open-addressing table: bucket -> newest point
+  std::vector<int> heads_;
+  size_t used_ = 0;
   std::vector<int> special_;
 };
 
 void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out* paths,
                  const double* x, phc_solve_result* res) {
   phc_solve_counts& c = res->counts;
-  PointSet sols(n, o.dedup_tol), ssols(n, o.singular_dedup_tol);
+  PointSet sols(n, o.dedup_tol, npaths), ssols(n, o.singular_dedup_tol, npaths);
   std::vector<int> mult;
   for (int64_t k = 0; k < npaths; ++k) {
     phc_path_out& p = paths[k];
