@@ -91,6 +91,35 @@ def cpu_paths_per_s(min_seconds=3.0, max_reps=50):
     return npaths * reps / el, threads, f"all {npaths} paths x {reps} solves, {threads} threads", el
 
 
+def cpu_serving_baseline(nsys_max=512, max_seconds=10.0):
+    """The serving stream on the host cores: the C++ restatement of the
+    reference solves one system per thread (each solve single-threaded, the
+    systems spread over all cores), over the first systems of the stream
+    until about max_seconds have passed."""
+    import concurrent.futures as cf
+    from oracle import oracle as O
+    from polyhomocont_b200 import workloads as W
+    O.build()
+    threads = os.cpu_count() or 1
+    systems = [W.build(lambda: O.SparseSystem(fast=True), *W.stream_system(i))
+               for i in range(nsys_max)]
+    done = paths = 0
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        for i0 in range(0, nsys_max, threads):
+            batch = systems[i0:i0 + threads]
+            for res, st in ex.map(lambda s: O.solve(s, nthreads=1), batch):
+                done += 1
+                paths += res.npaths
+            if time.perf_counter() - t0 >= max_seconds:
+                break
+    el = time.perf_counter() - t0
+    return {"systems_per_s": done / el, "paths_per_s": paths / el, "cores": threads,
+            "kind": "port",
+            "sample": f"first {done} systems of the stream, one system per thread, "
+                      f"{threads} threads (C++ restatement of the reference, -O3)"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -404,6 +433,8 @@ def main():
     serve = None
     if args.serving_systems > 0 and rank == 0:
         serve = serving(P, W, args.serving_systems, local)
+        if not args.no_cpu and world == 1:
+            serve["cpu_baseline"] = cpu_serving_baseline()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
