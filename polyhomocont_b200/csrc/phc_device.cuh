@@ -284,9 +284,7 @@ struct WarpWS {
   cf* pwf;    // power table, FP32 (mixed precision only)
   cd* jd;     // Jacobian of F^h, row-major, stride S
   cf* jf;
-  cd* prow;   // double-buffered pivot row (FP32 rows use it as cf*)
   int* piv;   // pivot row (lane) of each column
-  cd* sink;   // per-lane scratch for the schedule's non-final stores
 };
 
 template <typename T> __device__ __forceinline__ cpx<T>* ws_pw(const WarpWS& w);

@@ -59,7 +59,7 @@ int device_sms(int device);
 bool tuned_launch(int device, int precision, int schedule, int nm, int* warps, int* chunk);
 // Resolves the launch configuration for a plan on a device.
 int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, LaunchCfg* cfg);
-// Launches the tracking kernel (phc_kernels.cu).
+// Launches the tracking kernel (phc_launch.cu).
 cudaError_t launch_track(const LaunchCfg& cfg, const KParams& kp, int grid, cudaStream_t s);
 // Occupancy (blocks per SM) of the kernel for a configuration.
 int track_blocks_per_sm(const LaunchCfg& cfg);

@@ -1,6 +1,6 @@
 // phc_internal.h -- layout of the device-side system table ("plan") and
 // of the kernel parameters, shared by the host plan builder
-// (phc_plan.cpp) and the CUDA kernels (phc_kernels.cu).
+// (phc_plan.cpp) and the CUDA kernels (phc_track.cuh, phc_launch.cu).
 //
 // The reference evaluates F^h and its Jacobian per term with prefix and
 // suffix products over all N variables (eval_terms, src/sparse.f90:223-280).
@@ -174,7 +174,7 @@ struct alignas(16) WarpState {
 // Per-warp shared-memory workspace layout (byte offsets from the warp's
 // base), shared by host (sizing) and device (addressing).
 struct WsLayout {
-  int pwd, pwf, jd, jf, prow, piv, sink, st, bytes;
+  int pwd, pwf, jd, jf, piv, st, bytes;
 };
 
 PHC_HD inline int align16(int x) { return (x + 15) & ~15; }
@@ -186,9 +186,7 @@ PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size, bool mixed) {
   L.pwf = off; off += mixed ? align16(pw_size * 8) : 0;
   L.jd = off; off += align16((n + 1) * S * 16);  // rows 0..n-1: dF^h, row n: patch
   L.jf = off; off += mixed ? align16((n + 1) * S * 8) : 0;
-  L.prow = off; off += 2 * (kMaxN + 8) * 16;  // double-buffered pivot row, rhs, 1/pivot
   L.piv = off; off += kWarp * 4;
-  L.sink = off; off += kWarp * 16;
   L.st = off; off += align16((int)sizeof(WarpState));
   L.bytes = off;
   return L;

@@ -6,12 +6,11 @@
 // cauchy_endgame inside endpoint) are flattened into one warp-uniform
 // state machine whose every step either changes control state or runs
 // exactly one "unit": an evaluation of H(z,t) (and H_z, H_t), optionally
-// followed by a Gauss-Jordan solve (one right-hand side, or the columns of
-// the inverse for cond1). There is a single
-// call site of the unit per precision pair, so the elimination code exists
-// once per precision in the kernel binary, and the same machine
-// serves the predictor, the corrector, the end game's backward errors,
-// refine and cond1.
+// followed by a Gauss-Jordan solve (one right-hand side, or four columns
+// of the inverse for cond1). The unit has a single call site and chooses
+// its precision at run time, so each evaluation and elimination exists
+// once in the kernel binary, and the same machine serves the predictor,
+// the corrector, the end game's backward errors, refine and cond1.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -889,9 +888,7 @@ __device__ __forceinline__ WarpWS warp_workspace(const PlanHeader& P, unsigned c
   ws.pwf = reinterpret_cast<cf*>(wbase + L.pwf);
   ws.jd = reinterpret_cast<cd*>(wbase + L.jd);
   ws.jf = reinterpret_cast<cf*>(wbase + L.jf);
-  ws.prow = reinterpret_cast<cd*>(wbase + L.prow);
   ws.piv = reinterpret_cast<int*>(wbase + L.piv);
-  ws.sink = reinterpret_cast<cd*>(wbase + L.sink);
   *st = reinterpret_cast<WarpState*>(wbase + L.st);
   return ws;
 }
