@@ -221,10 +221,12 @@ NCU_DRAM_BYTES_PER_LAUNCH = 158464
 SCHED_NAMES = {0: "grid", 1: "persistent"}
 
 
-def serving(P, W, nsys, device, load=0.7):
+def serving(P, W, nsys, device, load=0.7, nslots=16, max_batch_systems=64,
+            max_batch_paths=1 << 15):
     systems = [W.build(P.SparseSystem, *W.stream_system(i)) for i in range(nsys)]
     npaths = sum(s.bezout() for s in systems)
-    cfg = dict(device=device, nslots=16, max_batch_systems=64, max_batch_paths=1 << 15)
+    cfg = dict(device=device, nslots=nslots, max_batch_systems=max_batch_systems,
+               max_batch_paths=max_batch_paths)
 
     def drain(srv, tickets):
         lat = []

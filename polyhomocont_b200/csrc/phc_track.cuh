@@ -51,23 +51,57 @@ constexpr int kCondChunk = 4;
 // footprint of the mixed kernel close to that of the FP64 kernel.
 // UK_COND eliminates against the unit vectors e_c0 .. e_c0+3 (cond1,
 // src/linalg.f90:135-174); the state machine runs one such unit per chunk.
+// Rows of up to 16 columns use the split layout (two lanes per row, half
+// a row each: evaluate_split, gauss_jordan_split); wider rows one lane per
+// row.
+template <int NM>
+struct RowLayout {
+  static constexpr bool kSplit = NM <= 16;
+  static constexpr int kRegs = kSplit ? NM / 2 : NM;  // complex values per lane
+};
+
+template <int NM, typename T>
+__device__ __forceinline__ void evaluate_rows(const WarpConst& C, const WarpWS& ws, cd z, cd t,
+                                              int lane, cpx<T> (&a)[RowLayout<NM>::kRegs],
+                                              cd& h, cd& ht) {
+  if constexpr (RowLayout<NM>::kSplit)
+    evaluate_split<NM / 2, T>(C, ws, z, t, lane, a, h, ht);
+  else
+    evaluate<NM, T>(C, ws, z, t, lane, a, h, ht);
+}
+
+template <int NM, int R, typename T>
+__device__ __forceinline__ bool eliminate(cpx<T> (&a)[RowLayout<NM>::kRegs], cpx<T> (&r)[R], int N,
+                                          int lane, int* piv) {
+  if constexpr (RowLayout<NM>::kSplit)
+    return gauss_jordan_split<NM / 2, R, T>(a, r, N, lane, piv);
+  else
+    return gauss_jordan<NM, R, T>(a, r, N, lane, piv);
+}
+
 template <int NM, bool MIXED>
 __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, int kind, int prec,
                                          int c0, cd zin, cd t, cd dt, int lane, UnitRes& u) {
+  using L = RowLayout<NM>;
+  constexpr int RW = L::kRegs;
   const int N = C.N;
+  // the row this lane works on, and whether it reports it (one lane per row)
+  const int row = L::kSplit ? (lane & 15) : lane;
+  const bool owner = L::kSplit ? lane < 16 : true;
   cd h, ht;
-  cpx<float> as[NM];
+  cpx<float> as[RW];
   if (!MIXED || prec != 1) {
-    cpx<double> a[NM];
-    evaluate<NM, double>(C, ws, zin, t, lane, a, h, ht);
+    cpx<double> a[RW];
+    evaluate_rows<NM, double>(C, ws, zin, t, lane, a, h, ht);
     if (kind == UK_BACKERR) {
       // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
       // absolute row sum of H_z
       double rs = 0.0;
 #pragma unroll
-      for (int j = 0; j < NM; ++j) rs += cabs(a[j]);
-      u.a1 = warp_max_nonneg(lane < N ? cabs(h) : 0.0);
-      u.a2 = warp_max_nonneg(lane < N ? rs : 0.0);
+      for (int j = 0; j < RW; ++j) rs += cabs(a[j]);
+      if constexpr (L::kSplit) rs += __shfl_xor_sync(kFull, rs, 16);
+      u.a1 = warp_max_nonneg(row < N ? cabs(h) : 0.0);
+      u.a2 = warp_max_nonneg(row < N ? rs : 0.0);
       u.ok = true;
       return;
     }
@@ -76,23 +110,27 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
       if (c0 == 0) {
         double anorm = 0.0;
 #pragma unroll
-        for (int j = 0; j < NM; ++j) {
-          if (j < N) anorm = fmax(anorm, warp_sum(lane < N ? cabs(a[j]) : 0.0));
+        for (int j = 0; j < RW; ++j) {
+          if constexpr (L::kSplit)
+            anorm = fmax(anorm, half_sum(row < N ? cabs(a[j]) : 0.0));
+          else if (j < N)
+            anorm = fmax(anorm, warp_sum(row < N ? cabs(a[j]) : 0.0));
         }
+        if constexpr (L::kSplit) anorm = warp_max_nonneg(anorm);
         u.a1 = anorm;
       }
       cd r[kCondChunk];
 #pragma unroll
       for (int q = 0; q < kCondChunk; ++q)
-        r[q] = (lane == c0 + q) ? cone<double>() : czero<double>();
-      if (!gauss_jordan<NM, kCondChunk, double>(a, r, N, lane, ws.piv)) {
+        r[q] = (row == c0 + q) ? cone<double>() : czero<double>();
+      if (!eliminate<NM, kCondChunk, double>(a, r, N, lane, ws.piv)) {
         u.ok = false;  // cond1 of an exactly singular matrix
         return;
       }
       double ainv = 0.0;
 #pragma unroll
       for (int q = 0; q < kCondChunk; ++q) {
-        if (c0 + q < N) ainv = fmax(ainv, warp_sum(lane < N ? cabs(r[q]) : 0.0));
+        if (c0 + q < N) ainv = fmax(ainv, warp_sum(owner && row < N ? cabs(r[q]) : 0.0));
       }
       u.a2 = ainv;
       u.ok = true;
@@ -101,7 +139,7 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
     if (!MIXED || prec == 0) {
       cd r[1];
       r[0] = (kind == UK_TANGENT) ? -(ht * dt) : -h;
-      u.ok = gauss_jordan<NM, 1, double>(a, r, N, lane, ws.piv);
+      u.ok = eliminate<NM, 1, double>(a, r, N, lane, ws.piv);
       if (!u.ok) return;
       const cd x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
       u.x = (lane < N) ? x : czero<double>();
@@ -109,14 +147,14 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
     }
     // mixed corrector: FP64 residual, FP32 update
 #pragma unroll
-    for (int j = 0; j < NM; ++j) as[j] = ccast<float>(a[j]);
+    for (int j = 0; j < RW; ++j) as[j] = ccast<float>(a[j]);
   } else {
-    evaluate<NM, float>(C, ws, zin, t, lane, as, h, ht);
+    evaluate_rows<NM, float>(C, ws, zin, t, lane, as, h, ht);
   }
   if constexpr (MIXED) {
     cpx<float> r[1];
     r[0] = ccast<float>((kind == UK_TANGENT) ? -(ht * dt) : -h);
-    u.ok = gauss_jordan<NM, 1, float>(as, r, N, lane, ws.piv);
+    u.ok = eliminate<NM, 1, float>(as, r, N, lane, ws.piv);
     if (!u.ok) return;
     const cpx<float> x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
     u.x = (lane < N) ? ccast<double>(x) : czero<double>();
