@@ -199,13 +199,6 @@ template <typename T>
 __device__ __forceinline__ cpx<T> shfl_xor(cpx<T> v, int m) {
   return mkc<T>(__shfl_xor_sync(kFull, v.re, m), __shfl_xor_sync(kFull, v.im, m));
 }
-// Sum over the 16 lanes of each half-warp (every lane gets its half's sum).
-template <typename T>
-__device__ __forceinline__ T half_sum(T v) {
-#pragma unroll
-  for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
 
 // Maximum over the warp of a value v >= +0 (moduli). The bit patterns of
 // non-negative doubles order like the values, so the maximum is taken on
@@ -528,18 +521,39 @@ __device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, c
 }
 
 // ---- split rows (N <= 16) --------------------------------------------------
-// For systems of up to 16 unknowns two lanes share a row: lane i (< 16)
-// holds columns 0..H-1 of row i and lane i+16 columns H..2H-1 (H = NM/2).
-// A shuffle instruction then moves a different pivot-row element to each
-// half, and each lane updates, loads and holds half a row.
+// For systems of up to 16 unknowns S lanes share a row (S = 2 for N <= 16,
+// S = 4 for N <= 8): with RPW = 32/S rows per warp, lane L works on row
+// L % RPW and holds its columns [q*HS, (q+1)*HS), q = L / RPW. A shuffle
+// instruction then moves a different pivot-row element to each part, and
+// each lane updates, loads and holds a fraction of a row.
+
+// Sum over the S lanes that share a row (lanes i, i + RPW, ...).
+template <int S, typename T>
+__device__ __forceinline__ T row_sum(T v) {
+  if constexpr (S >= 4) v += __shfl_xor_sync(kFull, v, 8);
+  if constexpr (S >= 2) v += __shfl_xor_sync(kFull, v, 16);
+  return v;
+}
+template <int S, typename T>
+__device__ __forceinline__ cpx<T> row_csum(cpx<T> v) {
+  return mkc<T>(row_sum<S>(v.re), row_sum<S>(v.im));
+}
+// Sum over the RPW lanes of one part (a column of the matrix).
+template <int S, typename T>
+__device__ __forceinline__ T part_sum(T v) {
+#pragma unroll
+  for (int o = 16 / S; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
 
 // evaluate() for the split layout: same power table and schedule, the
-// assembly of row i = lane & 15 over the lane's half of the columns; the
-// Euler sum adds the two halves' partial sums.
-template <int H, typename T>
+// assembly of row L % RPW over the lane's part of the columns; the Euler
+// sum adds the parts' partial sums.
+template <int HS, int S, typename T>
 __device__ __forceinline__ void evaluate_split(const WarpConst& C, const WarpWS& ws, cd zl, cd t,
-                                               int lane, cpx<T> (&a)[H], cd& h, cd& ht) {
-  const int n = C.n, N = C.N, S = C.S;
+                                               int lane, cpx<T> (&a)[HS], cd& h, cd& ht) {
+  constexpr int RPW = 32 / S;
+  const int n = C.n, N = C.N, S_ = C.S;
   cpx<T>* pw = ws_pw<T>(ws);
   power_table<T>(C, pw, ccast<T>(zl), lane);
   __syncwarp();
@@ -554,14 +568,14 @@ __device__ __forceinline__ void evaluate_split(const WarpConst& C, const WarpWS&
   const cpx<T> gt = gamma * tt;
   const cpx<T> omt = mkc<T>(T(1) - tt.re, -tt.im);
   const cpx<T>* zrow = pw + N;  // z_j = pw[1*N + j]
-  const int i = lane & 15, j0 = (lane >> 4) * H;
+  const int i = lane & (RPW - 1), j0 = (lane / RPW) * HS;
   const bool eq = i < n;
   const int row = i < n ? i : n;
-  const cpx<T>* Jr = ws_j<T>(ws) + row * S;
+  const cpx<T>* Jr = ws_j<T>(ws) + row * S_;
   const cpx<T> sc = eq ? omt : (i == n ? cone<T>() : czero<T>());
   cpx<T> f0 = czero<T>(), f1 = czero<T>();
 #pragma unroll
-  for (int jj = 0; jj < H; ++jj) {
+  for (int jj = 0; jj < HS; ++jj) {
     const int j = j0 + jj;
     if (j < N) {
       const cpx<T> jij = lds(&Jr[j]);
@@ -575,11 +589,10 @@ __device__ __forceinline__ void evaluate_split(const WarpConst& C, const WarpWS&
     }
   }
   // the row's constants are held by lane i (WarpConst is per lane); the
-  // upper half reads them from its partner
+  // other parts read them from it
   const int deg = __shfl_sync(kFull, C.deg, i);
   const double inv_deg = __shfl_sync(kFull, C.inv_deg, i);
-  const cpx<T> fp = f0 + f1;
-  const cpx<T> f = (T)inv_deg * (fp + shfl_xor(fp, 16));
+  const cpx<T> f = (T)inv_deg * row_csum<S>(f0 + f1);
   const int dm1 = eq ? deg - 1 : 0;
   const cpx<T> zd1 = lds(&pw[dm1 * N + row]);
   const cpx<T> wd1 = lds(&pw[dm1 * N + n]);
@@ -591,7 +604,7 @@ __device__ __forceinline__ void evaluate_split(const WarpConst& C, const WarpWS&
   const cpx<T> dg = eq ? (dd * gt) * zd1 : czero<T>();
   const cpx<T> dw = eq ? (dd * (gt * bi)) * wd1 : czero<T>();
 #pragma unroll
-  for (int jj = 0; jj < H; ++jj) {
+  for (int jj = 0; jj < HS; ++jj) {
     if (j0 + jj == i) a[jj] = a[jj] + dg;
     if (j0 + jj == n) a[jj] = a[jj] - dw;
   }
@@ -686,42 +699,52 @@ __device__ __forceinline__ bool gauss_jordan(cpx<T> (&a)[NM], cpx<T> (&r)[R], in
   return true;
 }
 
-// Gauss-Jordan for the split layout (lane i: columns 0..H-1 of row i,
-// lane i+16: columns H..2H-1; both lanes of a row keep the right-hand
-// sides). Same pivoting, multipliers and order of operations per element
-// as gauss_jordan. Each step shifts the row left by one column across the
-// two halves: the lower lane's last column receives the upper lane's first
-// column (one exchange per step, which also gives the upper lane the
-// row's current pivot-column entry for the multiplier). The pivot search
-// runs on the lower lanes; piv[] receives lower-lane indices.
-template <int H, int R, typename T>
-__device__ __forceinline__ bool gauss_jordan_split(cpx<T> (&a)[H], cpx<T> (&r)[R], int N,
+// Gauss-Jordan for the split layout (S lanes per row, HS columns each;
+// every lane of a row keeps the right-hand sides). Same pivoting,
+// multipliers and order of operations per element as gauss_jordan. Each
+// step shifts the row left by one column across the parts: a part's last
+// column receives the next part's first column. The pivot search runs on
+// the lanes of part 0; piv[] receives their indices.
+template <int HS, int S, int R, typename T>
+__device__ __forceinline__ bool gauss_jordan_split(cpx<T> (&a)[HS], cpx<T> (&r)[R], int N,
                                                    int lane, int* piv) {
-  static_assert(H >= 2, "split rows need at least two columns per half");
-  const int i = lane & 15;
-  const bool lower = lane < 16;
-  const int hsrc = lane & 16;  // the pivot row's lane on this lane's half: p | hsrc
+  static_assert(HS >= 2, "split rows need at least two columns per part");
+  constexpr int RPW = 32 / S;
+  const int i = lane & (RPW - 1);
+  const int part = lane / RPW;
+  const bool first = part == 0;
+  const bool last = part == S - 1;
   bool done = false;
   int mystep = -1;
   cpx<T> myrinv = czero<T>();
-  // x: the partner's first column: for a lower lane the row's column H,
-  // for an upper lane the row's column 0 (the pivot column)
-  cpx<T> x = shfl_xor(a[0], 16);
-  cpx<T> m0 = lower ? a[0] : x;
-  cpx<T> bnd = lower ? x : czero<T>();
+  // m0: the row's column 0 (part 0's first column); bnd: the next part's
+  // first column (this part's next column after the shift)
+  auto exchange = [&](cpx<T>& m0, cpx<T>& bnd) {
+    if constexpr (S == 2) {
+      const cpx<T> x = shfl_xor(a[0], 16);
+      m0 = first ? a[0] : x;
+      bnd = first ? x : czero<T>();
+    } else {
+      m0 = shfl(a[0], i);
+      const cpx<T> x = shfl(a[0], (lane + RPW) & 31);
+      bnd = last ? czero<T>() : x;
+    }
+  };
+  cpx<T> m0, bnd;
+  exchange(m0, bnd);
   T d2 = m0.re * m0.re + m0.im * m0.im;
   unsigned kmax;
-  int p = pivot_lane(d2, lower && i < N, lane, kmax);
+  int p = pivot_lane(d2, first && i < N, lane, kmax);
   T rd = rcp_nr(d2);
   for (int k = 0; k < N; ++k) {
-    const bool cand = lower && i < N && !done;
+    const bool cand = first && i < N && !done;
     cpx<T> rinv = mkc<T>(m0.re * rd, -m0.im * rd);
     if (kmax == 0u) {
       T km;
       p = warp_argmax_first(cand ? cabs(m0) : T(0), cand, km);
       if (!(km > T(0))) return false;
     }
-    const bool isrow = (i == p);  // p is a lower lane: row p
+    const bool isrow = (i == p);  // p is a lane of part 0: row p
     if (isrow && !(d2 >= T(1e-36) && d2 <= T(1e36))) rinv = crcp(m0);  // |p|^2 out of range
     if (isrow) {
       done = true;
@@ -731,22 +754,21 @@ __device__ __forceinline__ bool gauss_jordan_split(cpx<T> (&a)[H], cpx<T> (&r)[R
     const cpx<T> rp = shfl(rinv, p);
     // multiplier; the pivot row only shifts (l = 0)
     const cpx<T> l = isrow ? czero<T>() : m0 * rp;
-    // the pivot row's column H before the step (its upper lane's a[0])
-    const cpx<T> pb = shfl(a[0], p | 16);
-    const int src = p | hsrc;
+    // the pivot row's part, and its next part's first column, before the step
+    const int src = p + part * RPW;
+    const cpx<T> pb = shfl(a[0], (src + RPW) & 31);
     // next pivot column first, then the exchange and the next search
     a[0] = cfms(a[1], l, shfl(a[1], src));
-    x = shfl_xor(a[0], 16);
-    const cpx<T> m0n = lower ? a[0] : x;
-    const cpx<T> bndn = lower ? x : czero<T>();
+    cpx<T> m0n, bndn;
+    exchange(m0n, bndn);
     d2 = m0n.re * m0n.re + m0n.im * m0n.im;
-    const int pn = pivot_lane(d2, lower && i < N && !done, lane, kmax);
+    const int pn = pivot_lane(d2, first && i < N && !done, lane, kmax);
     rd = rcp_nr(d2);
 #pragma unroll
-    for (int jj = 1; jj + 1 < H; ++jj) a[jj] = cfms(a[jj + 1], l, shfl(a[jj + 1], src));
-    // the last column of the lower half comes from the upper half; the
-    // upper half's last column (beyond column 2H-1) is zero
-    a[H - 1] = lower ? cfms(bnd, l, pb) : czero<T>();
+    for (int jj = 1; jj + 1 < HS; ++jj) a[jj] = cfms(a[jj + 1], l, shfl(a[jj + 1], src));
+    // the part's last column comes from the next part; the last part's
+    // (beyond the row) is zero
+    a[HS - 1] = last ? czero<T>() : cfms(bnd, l, pb);
 #pragma unroll
     for (int q = 0; q < R; ++q) r[q] = cfms(r[q], l, shfl(r[q], p));
     m0 = m0n;
@@ -755,7 +777,7 @@ __device__ __forceinline__ bool gauss_jordan_split(cpx<T> (&a)[H], cpx<T> (&r)[R
   }
 #pragma unroll
   for (int q = 0; q < R; ++q) r[q] = r[q] * myrinv;
-  if (mystep >= 0 && lower) piv[mystep] = lane;
+  if (mystep >= 0 && first) piv[mystep] = lane;
   __syncwarp();
   return true;
 }

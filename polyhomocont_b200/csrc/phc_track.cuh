@@ -56,8 +56,10 @@ constexpr int kCondChunk = 4;
 // row.
 template <int NM>
 struct RowLayout {
-  static constexpr bool kSplit = NM <= 16;
-  static constexpr int kRegs = kSplit ? NM / 2 : NM;  // complex values per lane
+  static constexpr int kLanes = NM <= 8 ? 4 : (NM <= 16 ? 2 : 1);  // lanes per row
+  static constexpr bool kSplit = kLanes > 1;
+  static constexpr int kRegs = kLanes == 4 ? 2 : (kLanes == 2 ? NM / 2 : NM);  // per lane
+  static constexpr int kRows = 32 / kLanes;  // rows per warp
 };
 
 template <int NM, typename T>
@@ -65,7 +67,7 @@ __device__ __forceinline__ void evaluate_rows(const WarpConst& C, const WarpWS& 
                                               int lane, cpx<T> (&a)[RowLayout<NM>::kRegs],
                                               cd& h, cd& ht) {
   if constexpr (RowLayout<NM>::kSplit)
-    evaluate_split<NM / 2, T>(C, ws, z, t, lane, a, h, ht);
+    evaluate_split<RowLayout<NM>::kRegs, RowLayout<NM>::kLanes, T>(C, ws, z, t, lane, a, h, ht);
   else
     evaluate<NM, T>(C, ws, z, t, lane, a, h, ht);
 }
@@ -74,7 +76,8 @@ template <int NM, int R, typename T>
 __device__ __forceinline__ bool eliminate(cpx<T> (&a)[RowLayout<NM>::kRegs], cpx<T> (&r)[R], int N,
                                           int lane, int* piv) {
   if constexpr (RowLayout<NM>::kSplit)
-    return gauss_jordan_split<NM / 2, R, T>(a, r, N, lane, piv);
+    return gauss_jordan_split<RowLayout<NM>::kRegs, RowLayout<NM>::kLanes, R, T>(a, r, N, lane,
+                                                                                piv);
   else
     return gauss_jordan<NM, R, T>(a, r, N, lane, piv);
 }
@@ -86,8 +89,8 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
   constexpr int RW = L::kRegs;
   const int N = C.N;
   // the row this lane works on, and whether it reports it (one lane per row)
-  const int row = L::kSplit ? (lane & 15) : lane;
-  const bool owner = L::kSplit ? lane < 16 : true;
+  const int row = lane & (L::kRows - 1);
+  const bool owner = lane < L::kRows;
   cd h, ht;
   cpx<float> as[RW];
   if (!MIXED || prec != 1) {
@@ -99,7 +102,7 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
       double rs = 0.0;
 #pragma unroll
       for (int j = 0; j < RW; ++j) rs += cabs(a[j]);
-      if constexpr (L::kSplit) rs += __shfl_xor_sync(kFull, rs, 16);
+      rs = row_sum<L::kLanes>(rs);
       u.a1 = warp_max_nonneg(row < N ? cabs(h) : 0.0);
       u.a2 = warp_max_nonneg(row < N ? rs : 0.0);
       u.ok = true;
@@ -112,7 +115,7 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
 #pragma unroll
         for (int j = 0; j < RW; ++j) {
           if constexpr (L::kSplit)
-            anorm = fmax(anorm, half_sum(row < N ? cabs(a[j]) : 0.0));
+            anorm = fmax(anorm, part_sum<L::kLanes>(row < N ? cabs(a[j]) : 0.0));
           else if (j < N)
             anorm = fmax(anorm, warp_sum(row < N ? cabs(a[j]) : 0.0));
         }
