@@ -730,9 +730,13 @@ __device__ __forceinline__ bool gauss_jordan_split(cpx<T> (&a)[HS], cpx<T> (&r)[
       bnd = last ? czero<T>() : x;
     }
   };
+  // The pivot search and the reciprocal run on the lanes of part 0, which
+  // hold the pivot column themselves; the exchange only feeds the other
+  // parts' multipliers and stays off that chain. (The other parts' rinv,
+  // myrinv and right-hand sides are never read: results come from part 0.)
   cpx<T> m0, bnd;
   exchange(m0, bnd);
-  T d2 = m0.re * m0.re + m0.im * m0.im;
+  T d2 = first ? a[0].re * a[0].re + a[0].im * a[0].im : T(0);
   unsigned kmax;
   int p = pivot_lane(d2, first && i < N, lane, kmax);
   T rd = rcp_nr(d2);
@@ -745,7 +749,7 @@ __device__ __forceinline__ bool gauss_jordan_split(cpx<T> (&a)[HS], cpx<T> (&r)[
       if (!(km > T(0))) return false;
     }
     const bool isrow = (i == p);  // p is a lane of part 0: row p
-    if (isrow && !(d2 >= T(1e-36) && d2 <= T(1e36))) rinv = crcp(m0);  // |p|^2 out of range
+    if (isrow && first && !(d2 >= T(1e-36) && d2 <= T(1e36))) rinv = crcp(m0);  // |p|^2 out of range
     if (isrow) {
       done = true;
       mystep = k;
@@ -759,11 +763,11 @@ __device__ __forceinline__ bool gauss_jordan_split(cpx<T> (&a)[HS], cpx<T> (&r)[
     const cpx<T> pb = shfl(a[0], (src + RPW) & 31);
     // next pivot column first, then the exchange and the next search
     a[0] = cfms(a[1], l, shfl(a[1], src));
-    cpx<T> m0n, bndn;
-    exchange(m0n, bndn);
-    d2 = m0n.re * m0n.re + m0n.im * m0n.im;
+    d2 = first ? a[0].re * a[0].re + a[0].im * a[0].im : T(0);
     const int pn = pivot_lane(d2, first && i < N && !done, lane, kmax);
     rd = rcp_nr(d2);
+    cpx<T> m0n, bndn;
+    exchange(m0n, bndn);
 #pragma unroll
     for (int jj = 1; jj + 1 < HS; ++jj) a[jj] = cfms(a[jj + 1], l, shfl(a[jj + 1], src));
     // the part's last column comes from the next part; the last part's
