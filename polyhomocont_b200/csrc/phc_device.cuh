@@ -454,17 +454,16 @@ template <> __device__ __forceinline__ const cf* plan_coef<float>(const unsigned
 // and h_i, ht_i. F^h_i is obtained from row i of its Jacobian by Euler's
 // relation for homogeneous polynomials, F^h_i = (1/d_i) sum_j z_j dF^h_i/dz_j,
 // which needs no evaluation of its own.
-template <int NM, typename T>
+// F: the schedule form the kernel was compiled for (1: every record has at
+// most one power-table factor, 3: up to three).
+template <int NM, typename T, int F>
 __device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, cd zl, cd t,
                                          int lane, cpx<T> (&a)[NM], cd& h, cd& ht) {
   const int n = C.n, N = C.N, S = C.S;
   cpx<T>* pw = ws_pw<T>(ws);
   power_table<T>(C, pw, ccast<T>(zl), lane);
   __syncwarp();
-  if (C.max_fac <= 1)
-    run_schedule<T, 1>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws));
-  else
-    run_schedule<T, 3>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws));
+  run_schedule<T, F>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws));
   __syncwarp();
 
   const cpx<T> gamma = ccast<T>(C.gamma);
@@ -549,7 +548,7 @@ __device__ __forceinline__ T part_sum(T v) {
 // evaluate() for the split layout: same power table and schedule, the
 // assembly of row L % RPW over the lane's part of the columns; the Euler
 // sum adds the parts' partial sums.
-template <int HS, int S, typename T>
+template <int HS, int S, typename T, int F>
 __device__ __forceinline__ void evaluate_split(const WarpConst& C, const WarpWS& ws, cd zl, cd t,
                                                int lane, cpx<T> (&a)[HS], cd& h, cd& ht) {
   constexpr int RPW = 32 / S;
@@ -557,10 +556,7 @@ __device__ __forceinline__ void evaluate_split(const WarpConst& C, const WarpWS&
   cpx<T>* pw = ws_pw<T>(ws);
   power_table<T>(C, pw, ccast<T>(zl), lane);
   __syncwarp();
-  if (C.max_fac <= 1)
-    run_schedule<T, 1>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws));
-  else
-    run_schedule<T, 3>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws));
+  run_schedule<T, F>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws));
   __syncwarp();
 
   const cpx<T> gamma = ccast<T>(C.gamma);

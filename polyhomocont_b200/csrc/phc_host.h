@@ -16,6 +16,7 @@ namespace phc {
 struct HostPlan {
   std::vector<unsigned char> bytes;  // PlanHeader + records
   int n = 0, N = 0, S = 0, maxexp = 0, pw_size = 0, nrec = 0;
+  int max_fac = 0;  // most power-table factors of a Jacobian record
   int64_t nstart = 0;
 };
 
@@ -43,6 +44,7 @@ int homotopy_init(const phc_system* sys, int seed, HostHomotopy* h);
 struct LaunchCfg {
   int nm = 0;          // register-row capacity
   int precision = 0;   // PHC_PREC_*
+  int fac = 1;         // schedule form of the kernel: 1 or 3 factors per record
   int warps = 4;       // warps per block
   int persistent = 0;
   int chunk = 1;
@@ -64,9 +66,11 @@ cudaError_t launch_track(const LaunchCfg& cfg, const KParams& kp, int grid, cuda
 // Occupancy (blocks per SM) of the kernel for a configuration.
 int track_blocks_per_sm(const LaunchCfg& cfg);
 // Batched kernel (many systems per launch) and its occupancy.
-cudaError_t launch_track_batch(int nm, int prec, int warps, int smem, const KParamsBatch& kb,
-                               int grid, cudaStream_t s);
-int track_batch_blocks_per_sm(int nm, int prec, int warps, int smem);
+cudaError_t launch_track_batch(int nm, int prec, int fac, int warps, int smem,
+                               const KParamsBatch& kb, int grid, cudaStream_t s);
+int track_batch_blocks_per_sm(int nm, int prec, int fac, int warps, int smem);
+// Kernel variant: bit 0 the precision, bit 1 the three-factor schedule.
+inline int kernel_mode(int prec, int fac) { return (prec == PHC_PREC_MIXED ? 1 : 0) | (fac > 1 ? 2 : 0); }
 
 KOpts make_kopts(const phc_solve_options& so, const phc_gpu_options& g);
 phc_gpu_options gpu_defaults();

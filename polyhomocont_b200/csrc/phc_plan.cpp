@@ -293,6 +293,7 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   out->pw_size = pw_size + n_pre;
   out->nstart = radix;
   out->nrec = nrec;
+  out->max_fac = max_fac;
   return PHC_OK;
 }
 

@@ -170,7 +170,7 @@ int launch_batch(phc_server* S, Slot& s) {
   s.bytes = bytes;
   unsigned char* dev = static_cast<unsigned char*>(s.dbuf);
   const int prec = (g.precision == PHC_PREC_MIXED) ? PHC_PREC_MIXED : PHC_PREC_FP64;
-  int nm = 0, table_cap = 0, ws_cap = 0;
+  int nm = 0, table_cap = 0, ws_cap = 0, fac = 1;
   int64_t total = 0;
   BatchSys* d = reinterpret_cast<BatchSys*>(s.hbuf);
   size_t plan_end = up256(s.batch.size() * sizeof(BatchSys));
@@ -190,6 +190,7 @@ int launch_batch(phc_server* S, Slot& s) {
     d[i].opts = make_kopts(r.opts, g);
     total += r.npaths;
     nm = std::max(nm, r.cfg.nm);
+    fac = std::max(fac, r.cfg.fac);
     table_cap = std::max(table_cap, tb);
     ws_cap = std::max(ws_cap, align16(r.cfg.ws_bytes));
   }
@@ -202,7 +203,7 @@ int launch_batch(phc_server* S, Slot& s) {
     return PHC_ERR_UNSUPPORTED;
   }
   const int smem = warps * slice;
-  int bps = track_batch_blocks_per_sm(nm, prec, warps, smem);
+  int bps = track_batch_blocks_per_sm(nm, prec, fac, warps, smem);
   if (bps < 1) bps = 1;
   if (g.blocks_per_sm > 0) bps = std::min(bps, g.blocks_per_sm);
   KParamsBatch kb;
@@ -227,7 +228,7 @@ int launch_batch(phc_server* S, Slot& s) {
   if (e != cudaSuccess) return cuda_fail(e, "server H2D");
   e = cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long), s.stream);
   if (e != cudaSuccess) return cuda_fail(e, "server counter reset");
-  e = launch_track_batch(nm, prec, warps, smem, kb, grid, s.stream);
+  e = launch_track_batch(nm, prec, fac, warps, smem, kb, grid, s.stream);
   if (e != cudaSuccess) return cuda_fail(e, "server kernel launch");
   // each request's results are copied back as soon as its paths are done
   // (see engine_main); the event marks the end of the whole batch

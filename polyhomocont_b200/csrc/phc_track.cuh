@@ -62,14 +62,15 @@ struct RowLayout {
   static constexpr int kRows = 32 / kLanes;  // rows per warp
 };
 
-template <int NM, typename T>
+template <int NM, typename T, int F>
 __device__ __forceinline__ void evaluate_rows(const WarpConst& C, const WarpWS& ws, cd z, cd t,
                                               int lane, cpx<T> (&a)[RowLayout<NM>::kRegs],
                                               cd& h, cd& ht) {
   if constexpr (RowLayout<NM>::kSplit)
-    evaluate_split<RowLayout<NM>::kRegs, RowLayout<NM>::kLanes, T>(C, ws, z, t, lane, a, h, ht);
+    evaluate_split<RowLayout<NM>::kRegs, RowLayout<NM>::kLanes, T, F>(C, ws, z, t, lane, a, h,
+                                                                     ht);
   else
-    evaluate<NM, T>(C, ws, z, t, lane, a, h, ht);
+    evaluate<NM, T, F>(C, ws, z, t, lane, a, h, ht);
 }
 
 template <int NM, int R, typename T>
@@ -82,7 +83,7 @@ __device__ __forceinline__ bool eliminate(cpx<T> (&a)[RowLayout<NM>::kRegs], cpx
     return gauss_jordan<NM, R, T>(a, r, N, lane, piv);
 }
 
-template <int NM, bool MIXED>
+template <int NM, bool MIXED, int F>
 __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, int kind, int prec,
                                          int c0, cd zin, cd t, cd dt, int lane, UnitRes& u) {
   using L = RowLayout<NM>;
@@ -95,7 +96,7 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
   cpx<float> as[RW];
   if (!MIXED || prec != 1) {
     cpx<double> a[RW];
-    evaluate_rows<NM, double>(C, ws, zin, t, lane, a, h, ht);
+    evaluate_rows<NM, double, F>(C, ws, zin, t, lane, a, h, ht);
     if (kind == UK_BACKERR) {
       // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
       // absolute row sum of H_z
@@ -149,10 +150,12 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
       return;
     }
     // mixed corrector: FP64 residual, FP32 update
+    if constexpr (MIXED) {
 #pragma unroll
-    for (int j = 0; j < RW; ++j) as[j] = ccast<float>(a[j]);
+      for (int j = 0; j < RW; ++j) as[j] = ccast<float>(a[j]);
+    }
   } else {
-    evaluate_rows<NM, float>(C, ws, zin, t, lane, as, h, ht);
+    evaluate_rows<NM, float, F>(C, ws, zin, t, lane, as, h, ht);
   }
   if constexpr (MIXED) {
     cpx<float> r[1];
@@ -254,7 +257,7 @@ __device__ __forceinline__ double vnorm2(cd v, int lane, int N) {
 #define STV(f, v) sts(&LV(f), (v))
 
 // Tracks path k (1-based) and writes its record, z and x.
-template <int NM, int PREC>
+template <int NM, int PREC, int F>
 __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& C,
                                           const WarpWS& ws, WarpState& st, const KOpts& O,
                                           int64_t k, int lane, phc_path_out* rec, double* zo,
@@ -908,7 +911,8 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
       }
     }
     // ---- run the requested unit ----
-    run_unit<NM, kMixed>(C, ws, uk, kMixed ? u_prec : 0, st.cond_c0, zin, tin, dtin, lane, U);
+    run_unit<NM, kMixed, F>(C, ws, uk, kMixed ? u_prec : 0, st.cond_c0, zin, tin, dtin, lane,
+                            U);
     if (kMixed && u_prec == 0 && uk <= UK_NEWTON) ++st.c_retry;  // predictor/corrector unit in FP64
     ++st.units;
     pc = pc_after;
@@ -951,7 +955,7 @@ __device__ __forceinline__ void init_jacobian_buffer(const PlanHeader& P, const 
 }
 
 // Single-system kernel: every block stages the table once for its warps.
-template <int NM, int PREC>
+template <int NM, int PREC, int F>
 __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int tid = threadIdx.x;
@@ -988,7 +992,7 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
       qend = q + 1;
       if (q >= kp.count) break;
     }
-    track_one<NM, PREC>(P, C, ws, *stp, kp.opts, kp.k0 + q, lane, kp.out + q,
+    track_one<NM, PREC, F>(P, C, ws, *stp, kp.opts, kp.k0 + q, lane, kp.out + q,
                         kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
   }
 }
@@ -997,7 +1001,7 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
 // options) in one launch. Persistent warps pull global path indices from
 // one queue; a warp that moves on to another system stages that system's
 // table and options into its own shared-memory slice.
-template <int NM, int PREC>
+template <int NM, int PREC, int F>
 __global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1053,7 +1057,7 @@ __global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb)
     phc_path_out* out = reinterpret_cast<phc_path_out*>(kb.base + S.out_off) + kl;
     double* z = reinterpret_cast<double*>(kb.base + S.z_off) + 2 * kl * N;
     double* x = S.x_off >= 0 ? reinterpret_cast<double*>(kb.base + S.x_off) + 2 * kl * n : nullptr;
-    track_one<NM, PREC>(P, C, ws, *stp, *opts, kl + 1, lane, out, z, x);
+    track_one<NM, PREC, F>(P, C, ws, *stp, *opts, kl + 1, lane, out, z, x);
     if (kb.done != nullptr) {
       // every lane's result stores are made visible system-wide before the
       // path is counted as finished
@@ -1068,6 +1072,24 @@ __global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb)
 
 // Host-side launch and occupancy helpers of one register-row width NM,
 // defined in the instantiation units track_nm*.cu.
+// mode: bit 0 the precision (PHC_PREC_*), bit 1 the three-factor schedule
+#define PHC_FOR_MODES(MACRO, NMV, ...)                                            \
+  switch (mode) {                                                                 \
+    case 0: MACRO(NMV, PHC_PREC_FP64, 1, __VA_ARGS__); break;                     \
+    case 1: MACRO(NMV, PHC_PREC_MIXED, 1, __VA_ARGS__); break;                    \
+    case 2: MACRO(NMV, PHC_PREC_FP64, 3, __VA_ARGS__); break;                     \
+    default: MACRO(NMV, PHC_PREC_MIXED, 3, __VA_ARGS__); break;                   \
+  }
+#define PHC_SET_ATTR(NMV, PR, FF, smax)                                            \
+  cudaFuncSetAttribute(track_kernel<NMV, PR, FF>,                                 \
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, smax);        \
+  cudaFuncSetAttribute(track_batch_kernel<NMV, PR, FF>,                           \
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, smax)
+#define PHC_LAUNCH(NMV, PR, FF, K, P)                                              \
+  K<NMV, PR, FF><<<grid, block, smem, s>>>(P)
+#define PHC_OCC(NMV, PR, FF, K)                                                    \
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, K<NMV, PR, FF>, block, smem)
+
 #define PHC_DEFINE_NM(NMV)                                                        \
   namespace phc {                                                                 \
   static void set_smem_attr_##NMV() {                                             \
@@ -1077,55 +1099,37 @@ __global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb)
     if (dev >= 0 && dev < 64 && !done[dev]) {                                     \
       int smax = 0;                                                               \
       cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev); \
-      cudaFuncSetAttribute(track_kernel<NMV, PHC_PREC_FP64>,                      \
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
-      cudaFuncSetAttribute(track_kernel<NMV, PHC_PREC_MIXED>,                     \
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
-      cudaFuncSetAttribute(track_batch_kernel<NMV, PHC_PREC_FP64>,                \
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
-      cudaFuncSetAttribute(track_batch_kernel<NMV, PHC_PREC_MIXED>,               \
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, smax);    \
+      for (int mode = 0; mode < 4; ++mode) {                                      \
+        PHC_FOR_MODES(PHC_SET_ATTR, NMV, smax)                                    \
+      }                                                                           \
       done[dev] = 1;                                                              \
     }                                                                             \
   }                                                                               \
-  cudaError_t launch_nm_##NMV(int prec, const KParams& kp, int grid, int block,   \
+  cudaError_t launch_nm_##NMV(int mode, const KParams& kp, int grid, int block,   \
                               int smem, cudaStream_t s) {                         \
     set_smem_attr_##NMV();                                                        \
-    if (prec == PHC_PREC_MIXED)                                                   \
-      track_kernel<NMV, PHC_PREC_MIXED><<<grid, block, smem, s>>>(kp);            \
-    else                                                                          \
-      track_kernel<NMV, PHC_PREC_FP64><<<grid, block, smem, s>>>(kp);             \
+    PHC_FOR_MODES(PHC_LAUNCH, NMV, track_kernel, kp)                              \
     return cudaGetLastError();                                                    \
   }                                                                               \
-  cudaError_t launch_batch_nm_##NMV(int prec, const KParamsBatch& kb, int grid,     \
+  cudaError_t launch_batch_nm_##NMV(int mode, const KParamsBatch& kb, int grid,   \
                                     int block, int smem, cudaStream_t s) {       \
     set_smem_attr_##NMV();                                                        \
-    if (prec == PHC_PREC_MIXED)                                                   \
-      track_batch_kernel<NMV, PHC_PREC_MIXED><<<grid, block, smem, s>>>(kb);      \
-    else                                                                          \
-      track_batch_kernel<NMV, PHC_PREC_FP64><<<grid, block, smem, s>>>(kb);       \
+    PHC_FOR_MODES(PHC_LAUNCH, NMV, track_batch_kernel, kb)                        \
     return cudaGetLastError();                                                    \
   }                                                                               \
-  int occupancy_batch_nm_##NMV(int prec, int block, int smem) {                   \
+  int occupancy_batch_nm_##NMV(int mode, int block, int smem) {                   \
     set_smem_attr_##NMV();                                                        \
     int nb = 0;                                                                   \
-    cudaError_t e =                                                               \
-        (prec == PHC_PREC_MIXED)                                                  \
-            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(                      \
-                  &nb, track_batch_kernel<NMV, PHC_PREC_MIXED>, block, smem)      \
-            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(                      \
-                  &nb, track_batch_kernel<NMV, PHC_PREC_FP64>, block, smem);      \
+    cudaError_t e = cudaSuccess;                                                  \
+    PHC_FOR_MODES(PHC_OCC, NMV, track_batch_kernel)                               \
     return e == cudaSuccess ? nb : 0;                                             \
   }                                                                               \
-  int occupancy_nm_##NMV(int prec, int block, int smem) {                         \
+  int occupancy_nm_##NMV(int mode, int block, int smem) {                         \
     set_smem_attr_##NMV();                                                        \
     int nb = 0;                                                                   \
-    cudaError_t e =                                                               \
-        (prec == PHC_PREC_MIXED)                                                  \
-            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(                      \
-                  &nb, track_kernel<NMV, PHC_PREC_MIXED>, block, smem)            \
-            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(                      \
-                  &nb, track_kernel<NMV, PHC_PREC_FP64>, block, smem);            \
+    cudaError_t e = cudaSuccess;                                                  \
+    PHC_FOR_MODES(PHC_OCC, NMV, track_kernel)                                     \
     return e == cudaSuccess ? nb : 0;                                             \
   }                                                                               \
   }
+
