@@ -390,6 +390,32 @@ void engine_main(phc_server* S) {
 }  // namespace
 }  // namespace phc
 
+namespace phc {
+namespace {
+// Frees every CUDA resource of the server's slots (after its engine has
+// stopped, or when creation failed part way) and the server itself.
+void release_server(phc_server* S) {
+  cudaSetDevice(S->cfg.device);
+  for (auto& s : S->slots) {
+    if (s.stream) cudaStreamSynchronize(s.stream);
+    if (s.copy) cudaStreamSynchronize(s.copy);
+    if (s.dbuf && s.stream) cudaFreeAsync(s.dbuf, s.stream);
+    if (s.stream) cudaStreamSynchronize(s.stream);
+    if (s.hbuf) cudaFreeHost(s.hbuf);
+    if (s.counters) cudaFree(s.counters);
+    if (s.done) cudaEventDestroy(s.done);
+    for (auto ev : s.copied)
+      if (ev) cudaEventDestroy(ev);
+    if (s.done_h) cudaFreeHost(s.done_h);
+    if (s.copy) cudaStreamDestroy(s.copy);
+    if (s.stream) cudaStreamDestroy(s.stream);
+  }
+  for (void* h : S->retired_host) cudaFreeHost(h);
+  delete S;
+}
+}  // namespace
+}  // namespace phc
+
 extern "C" {
 
 int32_t phc_server_create(const phc_server_config* cfg, phc_server** out) {
@@ -401,45 +427,49 @@ int32_t phc_server_create(const phc_server_config* cfg, phc_server** out) {
     set_last_error("no CUDA device for the server");
     return PHC_ERR_NO_DEVICE;
   }
-  std::unique_ptr<phc_server> S(new (std::nothrow) phc_server());
+  phc_server* S = new (std::nothrow) phc_server();
   if (!S) return PHC_ERR_OOM;
+  // on any failure below, everything created so far is released
+  auto fail = [&](int st) {
+    release_server(S);
+    return st;
+  };
   S->cfg = *cfg;
   if (S->cfg.nslots < 1) S->cfg.nslots = 4;
   if (S->cfg.mem_budget_bytes <= 0) S->cfg.mem_budget_bytes = (int64_t)1 << 30;
   S->cfg.gpu.device = cfg->device;
   cudaError_t e = cudaSetDevice(cfg->device);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice"));
   S->slots.resize(S->cfg.nslots);
+  const int max_sys = S->cfg.max_batch_systems > 0 ? S->cfg.max_batch_systems : 256;
   for (auto& s : S->slots) {
     e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return cuda_fail(e, "server stream");
+    if (e != cudaSuccess) return fail(cuda_fail(e, "server stream"));
     e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
-    if (e != cudaSuccess) return cuda_fail(e, "server event");
+    if (e != cudaSuccess) return fail(cuda_fail(e, "server event"));
     e = cudaMalloc((void**)&s.counters, sizeof(unsigned long long));
-    if (e != cudaSuccess) return cuda_fail(e, "server counter");
+    if (e != cudaSuccess) return fail(cuda_fail(e, "server counter"));
     e = cudaStreamCreateWithFlags(&s.copy, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return cuda_fail(e, "server copy stream");
-    const int max_sys = S->cfg.max_batch_systems > 0 ? S->cfg.max_batch_systems : 256;
+    if (e != cudaSuccess) return fail(cuda_fail(e, "server copy stream"));
     e = cudaHostAlloc((void**)&s.done_h, (size_t)max_sys * sizeof(unsigned int),
                       cudaHostAllocMapped);
-    if (e != cudaSuccess) return cuda_fail(e, "server path counters");
+    if (e != cudaSuccess) return fail(cuda_fail(e, "server path counters"));
     std::memset(s.done_h, 0, (size_t)max_sys * sizeof(unsigned int));
     e = cudaHostGetDevicePointer((void**)&s.done_d, s.done_h, 0);
-    if (e != cudaSuccess) return cuda_fail(e, "server path counters (device view)");
+    if (e != cudaSuccess) return fail(cuda_fail(e, "server path counters (device view)"));
     s.copied.assign(max_sys, nullptr);
     for (auto& ev : s.copied) {
       e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-      if (e != cudaSuccess) return cuda_fail(e, "server copy event");
+      if (e != cudaSuccess) return fail(cuda_fail(e, "server copy event"));
     }
     // initial buffers sized for a typical batch, grown on demand
-    int st = grow(s, (size_t)1 << 22, S->retired_host);
-    if (st != PHC_OK) return st;
+    const int st = grow(s, (size_t)1 << 22, S->retired_host);
+    if (st != PHC_OK) return fail(st);
   }
   e = cudaDeviceSynchronize();
-  if (e != cudaSuccess) return cuda_fail(e, "server setup");
-  phc_server* raw = S.release();
-  raw->engine = std::thread(engine_main, raw);
-  *out = raw;
+  if (e != cudaSuccess) return fail(cuda_fail(e, "server setup"));
+  S->engine = std::thread(engine_main, S);
+  *out = S;
   return PHC_OK;
 }
 
@@ -573,23 +603,7 @@ int32_t phc_server_destroy(phc_server* S) {
   }
   S->cv.notify_all();
   if (S->engine.joinable()) S->engine.join();
-  cudaSetDevice(S->cfg.device);
-  for (auto& s : S->slots) {
-    if (s.stream) cudaStreamSynchronize(s.stream);
-    if (s.dbuf) cudaFreeAsync(s.dbuf, s.stream);
-    if (s.stream) cudaStreamSynchronize(s.stream);
-    if (s.hbuf) cudaFreeHost(s.hbuf);
-    if (s.counters) cudaFree(s.counters);
-    if (s.done) cudaEventDestroy(s.done);
-    if (s.copy) cudaStreamSynchronize(s.copy);
-    for (auto ev : s.copied)
-      if (ev) cudaEventDestroy(ev);
-    if (s.done_h) cudaFreeHost(s.done_h);
-    if (s.copy) cudaStreamDestroy(s.copy);
-    if (s.stream) cudaStreamDestroy(s.stream);
-  }
-  for (void* h : S->retired_host) cudaFreeHost(h);
-  delete S;
+  release_server(S);
   return PHC_OK;
 }
 
