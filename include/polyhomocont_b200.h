@@ -123,7 +123,10 @@ typedef struct {
   int32_t chunk;           /* persistent refill granularity (paths), 0 = the
                               tuned value, else 1                        */
   int32_t fp64_sticky;     /* mixed: FP64 steps after an FP32 failure, -1 = default */
-  int32_t pad_;
+  int32_t unit_budget_log2; /* per-path safety budget of 2^k units (evaluations
+                               with eliminations); a path that exhausts it ends
+                               with PHC_PATH_FAILED_MAX_STEPS. 0 = 2^24, far
+                               above any path tracked in practice; at most 40 */
 } phc_gpu_options;
 
 /* ---- per-path record: fields of type(path_result), src/solve.f90:86-119 -- */

@@ -62,7 +62,7 @@ class SolveOptions(ctypes.Structure):
 class GpuOptions(ctypes.Structure):
     _fields_ = [("precision", c_i32), ("schedule", c_i32), ("device", c_i32),
                 ("warps_per_block", c_i32), ("blocks_per_sm", c_i32), ("chunk", c_i32),
-                ("fp64_sticky", c_i32), ("pad_", c_i32)]
+                ("fp64_sticky", c_i32), ("unit_budget_log2", c_i32)]
 
 
 class SolveCounts(ctypes.Structure):

@@ -116,9 +116,10 @@ KOpts make_kopts(const phc_solve_options& so, const phc_gpu_options& g) {
   k.so = so;
   k.precision = g.precision;
   k.fp64_sticky = g.fp64_sticky < 0 ? 4 : g.fp64_sticky;
-  // safety budget of evaluate+LU units per path; far above any path the
-  // reference tracks in practice, it bounds every kernel's run time
-  k.max_units = (int64_t)1 << 24;
+  // safety budget of evaluate+LU units per path; by default far above any
+  // path the reference tracks in practice, it bounds every kernel's run time
+  const int lg = g.unit_budget_log2 > 0 ? std::min(g.unit_budget_log2, 40) : 24;
+  k.max_units = (int64_t)1 << lg;
   return k;
 }
 
