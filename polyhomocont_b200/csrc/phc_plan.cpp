@@ -99,6 +99,42 @@ void schedule(const std::vector<std::vector<Contribution>>& entries,
     load[best] += cost[e];
     lane_entries[best].push_back(e);
   }
+  // The kernel runs every lane for the longest lane's record count rounded
+  // up to a multiple of 4. If the LPT assignment misses the next lower
+  // multiple of 4, try to pack the entries into lanes of that many records
+  // (best fit, largest entries first); keep it when everything fits.
+  std::vector<long> recs(kWarp, 0);
+  for (int l = 0; l < kWarp; ++l)
+    for (int e : lane_entries[l]) recs[l] += (long)entries[e].size();
+  long total = 0, lpt_max = 0;
+  for (int l = 0; l < kWarp; ++l) {
+    total += recs[l];
+    lpt_max = std::max(lpt_max, recs[l]);
+  }
+  const long target = ((lpt_max + 3) & ~3L) - 4;
+  if (target > 0 && target * kWarp >= total) {
+    std::vector<int> by_size(order);
+    std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int b) {
+      return entries[a].size() > entries[b].size();
+    });
+    std::vector<long> fill(kWarp, 0);
+    std::vector<std::vector<int>> packed(kWarp);
+    bool ok = true;
+    for (int e : by_size) {
+      const long sz = (long)entries[e].size();
+      if (sz == 0) continue;
+      int best = -1;
+      for (int l = 0; l < kWarp; ++l)
+        if (fill[l] + sz <= target && (best < 0 || fill[l] > fill[best])) best = l;
+      if (best < 0) {
+        ok = false;
+        break;
+      }
+      fill[best] += sz;
+      packed[best].push_back(e);
+    }
+    if (ok) lane_entries.swap(packed);
+  }
   lanes.assign(kWarp, {});
   for (int l = 0; l < kWarp; ++l) {
     std::sort(lane_entries[l].begin(), lane_entries[l].end());
