@@ -205,7 +205,7 @@ int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, Lau
     return PHC_ERR_UNSUPPORTED;
   }
   cfg->precision = (g.precision == PHC_PREC_MIXED) ? PHC_PREC_MIXED : PHC_PREC_FP64;
-  cfg->fac = hp.max_fac <= 1 ? 1 : 3;
+  cfg->fac = hp.max_fac <= 1 ? 1 : (hp.max_fac == 2 ? 2 : 3);
   cfg->persistent = (g.schedule == PHC_SCHED_PERSISTENT) ? 1 : 0;
   int tw = 4, tc = 1;
   tuned_launch(device, cfg->precision, cfg->persistent, cfg->nm, &tw, &tc);

@@ -381,9 +381,9 @@ __device__ __forceinline__ void power_table(const WarpConst& C, cpx<T>* pw, cpx<
 // slot i*32 + lane of the coefficient and metadata arrays (layout in
 // phc_internal.h). A record multiplies its coefficient by up to three table
 // entries; F is the most any record of the system uses (an unused factor
-// is pw[0] = 1, exact), so a system whose records all have at most one
-// factor -- every quadratic system -- runs the one-factor form, which
-// loads and multiplies a third of the factors. Records do not depend on
+// is pw[0] = 1, exact), so a quadratic system (at most one factor per
+// record) runs the one-factor form and a cubic one the two-factor form,
+// which load and multiply only the factors they can have. Records do not depend on
 // each other except through the running sum, so consecutive records
 // overlap in the pipeline.
 template <typename T, int F>
@@ -396,7 +396,7 @@ __device__ __forceinline__ void run_schedule(const cpx<T>* __restrict__ coef,
   // the loads of a batch are issued together, then the products, then the
   // running sums. The sum is stored (a predicated store, not a branch) when
   // the record is the entry's last contribution.
-  static_assert(F == 1 || F == 3, "one- and three-factor schedules");
+  static_assert(F >= 1 && F <= 3, "one-, two- and three-factor schedules");
   cpx<T> acc = czero<T>();
   for (int i0 = 0; i0 < len; i0 += 4) {
     uint2 m[4];
@@ -416,16 +416,16 @@ __device__ __forceinline__ void run_schedule(const cpx<T>* __restrict__ coef,
     for (int u = 0; u < 4; ++u) {
       const unsigned lo = m[u].x, hi = m[u].y;
       p0[u] = lds(&pw[(lo >> 15) & 0x3ffu]);
-      if constexpr (F == 3) {
-        p1[u] = lds(&pw[(lo >> 25) | ((hi & 7u) << 7)]);
-        p2[u] = lds(&pw[(hi >> 3) & 0x3ffu]);
-      }
+      if constexpr (F >= 2) p1[u] = lds(&pw[(lo >> 25) | ((hi & 7u) << 7)]);
+      if constexpr (F == 3) p2[u] = lds(&pw[(hi >> 3) & 0x3ffu]);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       cpx<T> v;
       if constexpr (F == 1)
         v = c[u] * p0[u];
+      else if constexpr (F == 2)
+        v = (c[u] * p0[u]) * p1[u];
       else
         v = (c[u] * p0[u]) * (p1[u] * p2[u]);
       const unsigned lo = m[u].x;
@@ -454,8 +454,8 @@ template <> __device__ __forceinline__ const cf* plan_coef<float>(const unsigned
 // and h_i, ht_i. F^h_i is obtained from row i of its Jacobian by Euler's
 // relation for homogeneous polynomials, F^h_i = (1/d_i) sum_j z_j dF^h_i/dz_j,
 // which needs no evaluation of its own.
-// F: the schedule form the kernel was compiled for (1: every record has at
-// most one power-table factor, 3: up to three).
+// F: the schedule form the kernel was compiled for (the most power-table
+// factors of any record: 1, 2 or 3).
 template <int NM, typename T, int F>
 __device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, cd zl, cd t,
                                          int lane, cpx<T> (&a)[NM], cd& h, cd& ht) {

@@ -44,7 +44,7 @@ int homotopy_init(const phc_system* sys, int seed, HostHomotopy* h);
 struct LaunchCfg {
   int nm = 0;          // register-row capacity
   int precision = 0;   // PHC_PREC_*
-  int fac = 1;         // schedule form of the kernel: 1 or 3 factors per record
+  int fac = 1;         // schedule form of the kernel: 1, 2 or 3 factors per record
   int warps = 4;       // warps per block
   int persistent = 0;
   int chunk = 1;
@@ -69,8 +69,12 @@ int track_blocks_per_sm(const LaunchCfg& cfg);
 cudaError_t launch_track_batch(int nm, int prec, int fac, int warps, int smem,
                                const KParamsBatch& kb, int grid, cudaStream_t s);
 int track_batch_blocks_per_sm(int nm, int prec, int fac, int warps, int smem);
-// Kernel variant: bit 0 the precision, bit 1 the three-factor schedule.
-inline int kernel_mode(int prec, int fac) { return (prec == PHC_PREC_MIXED ? 1 : 0) | (fac > 1 ? 2 : 0); }
+// Kernel variant: bit 0 the precision, mode / 2 the schedule form (1, 2, 3
+// factors per record).
+inline int kernel_mode(int prec, int fac) {
+  const int f = fac <= 1 ? 0 : (fac == 2 ? 1 : 2);
+  return (prec == PHC_PREC_MIXED ? 1 : 0) + 2 * f;
+}
 
 KOpts make_kopts(const phc_solve_options& so, const phc_gpu_options& g);
 phc_gpu_options gpu_defaults();

@@ -1072,12 +1072,14 @@ __global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb)
 
 // Host-side launch and occupancy helpers of one register-row width NM,
 // defined in the instantiation units track_nm*.cu.
-// mode: bit 0 the precision (PHC_PREC_*), bit 1 the three-factor schedule
+// mode: bit 0 the precision (PHC_PREC_*), mode / 2 + 1 the schedule form
 #define PHC_FOR_MODES(MACRO, NMV, ...)                                            \
   switch (mode) {                                                                 \
     case 0: MACRO(NMV, PHC_PREC_FP64, 1, __VA_ARGS__); break;                     \
     case 1: MACRO(NMV, PHC_PREC_MIXED, 1, __VA_ARGS__); break;                    \
-    case 2: MACRO(NMV, PHC_PREC_FP64, 3, __VA_ARGS__); break;                     \
+    case 2: MACRO(NMV, PHC_PREC_FP64, 2, __VA_ARGS__); break;                     \
+    case 3: MACRO(NMV, PHC_PREC_MIXED, 2, __VA_ARGS__); break;                    \
+    case 4: MACRO(NMV, PHC_PREC_FP64, 3, __VA_ARGS__); break;                     \
     default: MACRO(NMV, PHC_PREC_MIXED, 3, __VA_ARGS__); break;                   \
   }
 #define PHC_SET_ATTR(NMV, PR, FF, smax)                                            \
@@ -1099,7 +1101,7 @@ __global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb)
     if (dev >= 0 && dev < 64 && !done[dev]) {                                     \
       int smax = 0;                                                               \
       cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev); \
-      for (int mode = 0; mode < 4; ++mode) {                                      \
+      for (int mode = 0; mode < 6; ++mode) {                                      \
         PHC_FOR_MODES(PHC_SET_ATTR, NMV, smax)                                    \
       }                                                                           \
       done[dev] = 1;                                                              \
