@@ -219,6 +219,24 @@ void phc_sparse_degrees(const phc_sparse* s, int32_t* d);  /* :186-195 */
 /* view of the packed table; valid until the builder changes */
 int32_t phc_sparse_table(const phc_sparse* s, phc_system* out);
 
+/* ---- user-evaluator systems (class(poly_system), src/system.f90:27-67) -- */
+/* sys%evaluate(x, f, jac): x[2n], f[2n] interleaved complex; jac[2 n n] is
+ * the n x n Jacobian column-major, jac(i, j) = dF_i/dx_j at complex index
+ * i + j*n (Fortran's layout). Returns 0, or nonzero to abort sampling. */
+typedef int32_t (*phc_evaluator)(void* ctx, int32_t n, const double* x, double* f,
+                                 double* jac);
+/* Replaces the builder's content (sys%init(n) + n add_equation calls) with
+ * the sparse table of the polynomial system that eval computes, whose
+ * equation i has the exact total degree degrees[i]: F is sampled at
+ * 2 C(n+d, d) generic points per degree d and interpolated by least
+ * squares, and the table is checked against F and the Jacobian at fresh
+ * points (worst relative error in *max_error, may be NULL). Returns
+ * err_invalid_input when eval is not a polynomial of those degrees or its
+ * Jacobian disagrees, PHC_ERR_UNSUPPORTED above 1500 monomials of degree
+ * <= d_i, PHC_ERR_ABORTED when eval returned nonzero. */
+int32_t phc_sparse_sample(phc_sparse* s, int32_t n, const int32_t* degrees, phc_evaluator eval,
+                          void* ctx, int32_t seed, double* max_error);
+
 /* ---- homotopy set-up: gen%seed(seed); hom%init(sys, gen, status) ------- */
 /* src/random.f90:43-62, src/homotopy.f90:104-149. gamma[2], b[2n],
  * patch[2(n+1)] are caller-allocated; nstart = Bezout number. */

@@ -90,6 +90,12 @@ assert PATH_DTYPE.itemsize == 96
 _lib = {}
 
 
+# evaluate(x, f, jac) of a user system as a C callback (orc_user_evaluator)
+USER_EVALUATOR = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+                                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(ctypes.c_double))
+
+
 def build(fast=False):
     """Compile the restatement with make (both libraries)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -128,6 +134,7 @@ def lib(fast=False):
         "orc_sparse_table": (None, [vp, ip, ip, dp]),
         "orc_sparse_evaluate": (None, [vp, dp, dp, dp]),
         "orc_sparse_evaluate_homogeneous": (None, [vp, dp, dp, dp]),
+        "orc_sparse_set_user": (None, [vp, i32, ip, USER_EVALUATOR, vp]),
         "orc_hom_new": (vp, []), "orc_hom_free": (None, [vp]),
         "orc_hom_init": (i32, [vp, vp, vp]), "orc_hom_nstart": (i32, [vp]),
         "orc_hom_constants": (None, [vp, dp, dp, dp]),
@@ -283,6 +290,33 @@ class SparseSystem:
         jac = np.zeros((n, n + 1), dtype=np.complex128, order="F")
         self._L.orc_sparse_evaluate_homogeneous(self.h, _dp(z), _dp(f), _dp(jac))
         return f, jac
+
+
+class UserSystem(SparseSystem):
+    """A user system, class(poly_system) of src/system.f90:27-67: usys has
+    nvars(), degrees() and evaluate(x) -> (f, jac[i, j] = dF_i/dx_j). The
+    restatement evaluates F^h through the reference's default
+    homogenization (poly_system_evaluate_homogeneous, src/system.f90:71-119)
+    and solves it like any system; use nthreads=1 (the callback runs
+    Python)."""
+
+    def __init__(self, usys, fast=False):
+        super().__init__(fast=fast)
+        n = int(usys.nvars())
+        self._deg = np.ascontiguousarray(np.asarray(usys.degrees(), dtype=np.int32).ravel())
+
+        def cb(_ctx, m, xp, fp, jp):
+            x = np.ctypeslib.as_array(xp, shape=(2 * m,)).view(np.complex128).copy()
+            f, jac = usys.evaluate(x)
+            np.ctypeslib.as_array(fp, shape=(2 * m,))[:] = (
+                np.asarray(f, dtype=np.complex128).reshape(m).view(np.float64))
+            np.ctypeslib.as_array(jp, shape=(2 * m * m,))[:] = np.asfortranarray(
+                np.asarray(jac, dtype=np.complex128).reshape(m, m)).ravel(order="F").view(
+                    np.float64)
+            return 0
+
+        self._cb = USER_EVALUATOR(cb)
+        self._L.orc_sparse_set_user(self.h, n, _ip(self._deg), self._cb, None)
 
 
 class Homotopy:

@@ -20,6 +20,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <thread>
 #include <vector>
 
@@ -233,6 +234,10 @@ struct sparse_system {
   std::vector<int> exps;   // n x nt column-major
   std::vector<int> hexps;  // (n+1) x nt column-major
   cvec coefs;
+  // a user system (class(poly_system) other than sparse_system): F and
+  // dF/dx from a callback, homogenized by poly_system_evaluate_homogeneous
+  orc_user_evaluator user = nullptr;
+  void* user_ctx = nullptr;
   int nt() const { return (int)coefs.size(); }
 };
 
@@ -334,8 +339,41 @@ static void eval_terms(int neq, const int* first, const int* exps, int m,
 #undef PW
 }
 
+/* poly_system_evaluate_homogeneous, src/system.f90:71-119: the default
+ * homogenization of a user system, through x = z(1:n)/w and the affine
+ * evaluator; jac is n x (n+1) column-major. */
+static void user_evaluate_homogeneous(const sparse_system& s, const cx* z, cx* f, cx* jac,
+                                      eval_scratch& sc) {
+  const int n = s.n;
+  cvec& x = sc.pre;
+  cvec& fa = sc.suf;
+  cvec& ja = sc.pw;
+  x.resize(n);
+  fa.resize(n);
+  ja.resize((size_t)n * n);
+  cx w = z[n];
+  if (w == C(0.0))
+    w = C(std::numeric_limits<double>::epsilon() *
+          std::max(norm_inf(z, n + 1), std::numeric_limits<double>::min()));
+  for (int j = 0; j < n; ++j) x[j] = z[j] / w;
+  s.user(s.user_ctx, n, reinterpret_cast<const double*>(x.data()),
+         reinterpret_cast<double*>(fa.data()), reinterpret_cast<double*>(ja.data()));
+  for (int i = 0; i < n; ++i) {
+    const cx wd1 = cpowi(w, s.deg[i] - 1);
+    f[i] = wd1 * w * fa[i];
+    for (int j = 0; j < n; ++j) jac[i + (size_t)j * n] = wd1 * ja[i + (size_t)j * n];
+    cx acc = C(0.0);
+    for (int j = 0; j < n; ++j) acc = acc + x[j] * ja[i + (size_t)j * n];
+    jac[i + (size_t)n * n] = wd1 * (C((double)s.deg[i]) * fa[i] - acc);
+  }
+}
+
 static void sparse_evaluate_homogeneous(const sparse_system& s, const cx* z,
                                         cx* f, cx* jac, eval_scratch& sc) {
+  if (s.user) {
+    user_evaluate_homogeneous(s, z, f, jac, sc);
+    return;
+  }
   // src/sparse.f90:209-221
   eval_terms(s.neq, s.first.data(), s.hexps.data(), s.n + 1, s.coefs.data(),
              s.maxexp, z, f, jac, sc);
@@ -1183,6 +1221,16 @@ int32_t orc_solve_linear(int32_t n, const double* a, const double* b, double* x)
 double orc_cond1(int32_t n, const double* a) { return cond1(n, ccx(a)); }
 double orc_norm_inf(int32_t n, const double* z) { return norm_inf(ccx(z), n); }
 
+void orc_sparse_set_user(void* s, int32_t n, const int32_t* degrees, orc_user_evaluator fn,
+                         void* ctx) {
+  sparse_system& p = *static_cast<sparse_system*>(s);
+  sparse_init(p, n);
+  p.neq = n;
+  p.first.assign(n + 1, 0);
+  p.deg.assign(degrees, degrees + n);
+  p.user = fn;
+  p.user_ctx = ctx;
+}
 void* orc_sparse_new(void) { return new sparse_system(); }
 void orc_sparse_free(void* s) { delete static_cast<sparse_system*>(s); }
 void orc_sparse_init(void* s, int32_t n) { sparse_init(*static_cast<sparse_system*>(s), n); }

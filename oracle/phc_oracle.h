@@ -166,6 +166,14 @@ void orc_sparse_table(void* s, int32_t* first, int32_t* hexps, double* coefs);
 void orc_sparse_evaluate(void* s, const double* x, double* f, double* jac);
 void orc_sparse_evaluate_homogeneous(void* s, const double* z, double* f,
                                      double* jac);
+/* A user system (class(poly_system), src/system.f90:27-67): evaluate(x, f,
+ * jac) as a callback (x, f interleaved complex [n]; jac n x n column-major),
+ * exact degrees[n]. The object then evaluates F^h by the reference's default
+ * homogenization (src/system.f90:71-119) and solves like any system. */
+typedef int32_t (*orc_user_evaluator)(void* ctx, int32_t n, const double* x, double* f,
+                                      double* jac);
+void orc_sparse_set_user(void* s, int32_t n, const int32_t* degrees, orc_user_evaluator fn,
+                         void* ctx);
 
 /* ---- homotopy.f90 ---- */
 void* orc_hom_new(void);

@@ -4,6 +4,8 @@ Python mirror of the reference's Fortran API over the C ABI of
 libphc_b200.so (include/polyhomocont_b200.h):
 
     type(sparse_system)   -> SparseSystem   (init, add_equation, nvars, ...)
+    class(poly_system)    -> PolySystem     (nvars, degrees, evaluate; sampled
+                                             into a SparseSystem by sample_system)
     type(solve_options)   -> SolveOptions   (tracker, endgame, seed, tolerances)
     solve(sys, res, status, options) -> res, status = solve(sys, options)
     type(solve_result)    -> SolveResult    (paths, solutions, counts, ...)
@@ -127,6 +129,66 @@ class SparseSystem:
         return int(self._L.phc_bezout(ctypes.byref(t))) if st == 0 else 0
 
 
+class PolySystem:
+    """class(poly_system), src/system.f90:27-67: a user system given by
+    nvars(), degrees() (exact total degrees d_i >= 1) and evaluate(x) ->
+    (f, jac) with f = F(x) and jac[i, j] = dF_i/dx_j. solve() and
+    solve_paths() turn it into a sparse table (sample_system) and track
+    that on the GPU."""
+
+    def nvars(self):
+        raise NotImplementedError
+
+    def degrees(self):
+        raise NotImplementedError
+
+    def evaluate(self, x):
+        raise NotImplementedError
+
+
+def sample_system(sys, seed=1):
+    """phc_sparse_sample: the SparseSystem of the polynomial system that the
+    PolySystem sys evaluates. Returns (SparseSystem, status, max_error);
+    status is err_invalid_input when sys.evaluate is not a polynomial of
+    the stated degrees or its Jacobian disagrees with F, and max_error is
+    the worst relative error of the table against sys at the check points.
+    An exception raised by sys.evaluate is raised again here."""
+    n = int(sys.nvars())
+    deg = np.ascontiguousarray(np.asarray(sys.degrees(), dtype=np.int32).ravel())
+    if deg.size != n:
+        return SparseSystem(), ERR_INVALID_INPUT, 0.0
+    raised = []
+
+    def cb(_ctx, m, xp, fp, jp):
+        try:
+            x = np.ctypeslib.as_array(xp, shape=(2 * m,)).view(np.complex128)
+            f, jac = sys.evaluate(x.copy())
+            f = np.asarray(f, dtype=np.complex128).reshape(m)
+            jac = np.asarray(jac, dtype=np.complex128).reshape(m, m)
+            np.ctypeslib.as_array(fp, shape=(2 * m,))[:] = f.view(np.float64)
+            np.ctypeslib.as_array(jp, shape=(2 * m * m,))[:] = (
+                np.asfortranarray(jac).ravel(order="F").view(np.float64))
+            return 0
+        except Exception as e:  # noqa: BLE001 - re-raised after the call
+            raised.append(e)
+            return 1
+
+    s = SparseSystem()
+    err = ctypes.c_double(0.0)
+    fn = _abi.EVALUATOR(cb)
+    st = s._L.phc_sparse_sample(s.h, n, _abi.iptr(deg), fn, None, int(seed), ctypes.byref(err))
+    if raised:
+        raise raised[0]
+    return s, st, float(err.value)
+
+
+def _as_sparse(sys):
+    if isinstance(sys, SparseSystem):
+        return sys, PHC_OK
+    s, st, _ = sample_system(sys)
+    return s, st
+
+
 def encode_request(sys, options=None):
     """The system (and options, if given) in the compact request format of
     the serving path (phc_request_encode) as bytes."""
@@ -226,12 +288,15 @@ def _fill_result(n, npaths, bufs, rc):
 
 def solve(sys, options=None, gpu=None, buffers=None):
     """solve(sys, res, status, options), src/solve.f90:154-215, on the GPU.
-    Returns (res, status); status is err_invalid_input for systems the
+    sys is a SparseSystem or a PolySystem (sampled first). Returns (res, status); status is err_invalid_input for systems the
     reference rejects. Device errors raise PhcError. buffers: optional
     (bufs, rc) from _result_buffers, reused across calls."""
     L = _abi.lib()
     o = options if options is not None else default_options()
     g = gpu if gpu is not None else default_gpu_options()
+    sys, st = _as_sparse(sys)
+    if st != PHC_OK:
+        return SolveResult(), st
     t, st = sys.table()
     if st != PHC_OK:
         return SolveResult(), st
@@ -282,6 +347,9 @@ def solve_paths(sys, options=None, gpu=None, k0=1, count=None, seed=None):
     L = _abi.lib()
     o = options if options is not None else default_options()
     g = gpu if gpu is not None else default_gpu_options()
+    sys, st = _as_sparse(sys)
+    if st != PHC_OK:
+        return None, None, None, st
     gamma, b, patch, nstart, st = homotopy_init(sys, o.seed if seed is None else seed)
     if st != PHC_OK:
         return None, None, None, st

@@ -110,6 +110,9 @@ PATH_DTYPE = np.dtype([
     ("cond", "<f8"), ("residual", "<f8")])
 assert PATH_DTYPE.itemsize == 96
 
+# sys%evaluate(x, f, jac) as a C callback (phc_evaluator)
+EVALUATOR = ctypes.CFUNCTYPE(c_i32, c_vp, c_i32, P(c_dbl), P(c_dbl), P(c_dbl))
+
 # every entry point the header declares: (name, restype, argtypes)
 SIGNATURES = [
     ("phc_version", ctypes.c_char_p, []),
@@ -126,6 +129,7 @@ SIGNATURES = [
     ("phc_sparse_total_terms", c_i32, [c_vp]),
     ("phc_sparse_degrees", None, [c_vp, P(c_i32)]),
     ("phc_sparse_table", c_i32, [c_vp, P(SystemC)]),
+    ("phc_sparse_sample", c_i32, [c_vp, c_i32, P(c_i32), EVALUATOR, c_vp, c_i32, P(c_dbl)]),
     ("phc_homotopy_init", c_i32, [P(SystemC), c_i32, P(c_dbl), P(c_dbl), P(c_dbl),
                                   P(c_i64)]),
     ("phc_bezout", c_i64, [P(SystemC)]),
