@@ -191,8 +191,12 @@ def _as_sparse(sys):
 
 def encode_request(sys, options=None):
     """The system (and options, if given) in the compact request format of
-    the serving path (phc_request_encode) as bytes."""
+    the serving path (phc_request_encode) as bytes. sys is a SparseSystem
+    or a PolySystem (sampled first)."""
     L = _abi.lib()
+    sys, st = _as_sparse(sys)
+    if st != PHC_OK:
+        raise PhcError(st, "sample_system")
     t, st = sys.table()
     if st != PHC_OK:
         raise PhcError(st, "table")
@@ -560,7 +564,11 @@ class Server:
 
     def submit(self, sys, options=None):
         """Returns (ticket, status); status != 0 means the request was refused
-        (err_invalid_input, PHC_ERR_ADMISSION, ...)."""
+        (err_invalid_input, PHC_ERR_ADMISSION, ...). sys is a SparseSystem or
+        a PolySystem (sampled first; the server compiles its own copy)."""
+        sys, st = _as_sparse(sys)
+        if st != PHC_OK:
+            return None, st
         t, st = sys.table()
         if st != PHC_OK:
             return None, st

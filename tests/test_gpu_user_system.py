@@ -81,3 +81,34 @@ def test_user_system_parity(orc, name, precision):
         assert set_distance(got.solutions, ref.solutions) <= TOL_REGULAR
     if ref.nsingular:
         assert set_distance(got.singular_solutions, ref.singular_solutions) <= TOL_SINGULAR
+
+
+def test_user_systems_through_the_server():
+    """A user system submitted to the serving loop gives the same result as
+    solve() on it, also when mixed with sparse systems in one batch."""
+    users = [ClosedForm(), CircleCubic(), TermEvaluator(*W.katsura(3))]
+    others = [W.build(P.SparseSystem, *W.stream_system(400 + i)) for i in range(3)]
+    srv = P.Server(nslots=2, max_batch_systems=6)
+    try:
+        tickets = []
+        for u, o in zip(users, others):
+            for s in (u, o):
+                t, st = srv.submit(s)
+                assert st == 0
+                tickets.append((s, t))
+        for _, t in tickets:
+            assert srv.wait(t, 120000) == 0
+        got = [(s, srv.result(t)) for s, t in tickets]
+    finally:
+        srv.close()
+    for s, (res, st, _lat) in got:
+        alone, st2 = P.solve(s)
+        assert st == st2 == 0
+        for key in ("npaths", "nsolutions", "nreal", "nsingular", "ninfinite", "nfailed",
+                    "nduplicates"):
+            assert getattr(res, key) == getattr(alone, key), key
+        for key in ("status", "winding_number", "at_infinity", "singular", "is_real",
+                    "solution_index"):
+            assert np.array_equal(res.paths[key], alone.paths[key]), key
+        if alone.nsolutions:
+            assert set_distance(res.solutions, alone.solutions) <= TOL_REGULAR
