@@ -29,6 +29,7 @@ namespace phc {
 static thread_local std::string g_last_error;
 
 void set_last_error(const std::string& s) { g_last_error = s; }
+std::string last_error_text() { return g_last_error; }
 
 int cuda_fail(cudaError_t e, const char* what) {
   set_last_error(std::string(what) + ": " + cudaGetErrorString(e));

@@ -23,6 +23,9 @@ struct HostPlan {
 int validate_system(const phc_system* sys);
 int validate_options(const phc_solve_options* o);
 int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out);
+// Checks every index the kernels read from a compiled table (build_plan
+// calls it on its result); PHC_ERR_UNSUPPORTED with the reason otherwise.
+int verify_plan(const unsigned char* bytes, size_t size);
 
 // Homotopy constants drawn on the host with the reference generator.
 struct HostHomotopy {
@@ -81,6 +84,8 @@ phc_gpu_options gpu_defaults();
 phc_solve_options solve_defaults();
 
 void set_last_error(const std::string& s);
+// The calling thread's last error text (error texts are per thread).
+std::string last_error_text();
 int cuda_fail(cudaError_t e, const char* what);
 
 // Host bookkeeping of solve() (add_solution, add_singular, find,

@@ -7,6 +7,7 @@
 #include <map>
 #include <cstring>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "phc_host.h"
@@ -171,6 +172,104 @@ size_t max_len(const std::vector<std::vector<PackedRec>>& lanes) {
 
 }  // namespace
 
+// Every index the kernels read out of a compiled table, checked on the host
+// before the table is used: header sizes against the compile-time limits,
+// array offsets against the table's size, each record's destination and
+// power-table factors, the extended power-table levels (each entry built
+// only from entries that exist before its level runs), and that no two
+// records of a schedule finish the same entry. The kernels index shared
+// memory with these values unchecked, so a table that fails here would make
+// them read or write out of bounds; verify_plan turns that into an error
+// status instead. It runs after every table compile (O(records)).
+int verify_plan(const unsigned char* bytes, size_t size) {
+  auto fail = [](const char* what) {
+    set_last_error(std::string("table verification failed: ") + what);
+    return PHC_ERR_UNSUPPORTED;
+  };
+  if (bytes == nullptr || size < sizeof(PlanHeader)) return fail("short table");
+  PlanHeader H;
+  std::memcpy(&H, bytes, sizeof(H));
+  if (H.n < 1 || H.N != H.n + 1 || H.N > kMaxN) return fail("dimensions");
+  if (H.S < H.N || H.S % 2 == 0 || (int64_t)H.n * H.S > 1024) return fail("row stride");
+  if (H.maxexp < 1 || H.pw_size != (H.maxexp + 1) * H.N) return fail("power table size");
+  if (H.n_pre < 0 || H.pw_total != H.pw_size + H.n_pre || H.pw_total > kMaxPw)
+    return fail("extended power table size");
+  if (H.n_levels < 0 || H.n_levels > kMaxLevels) return fail("levels");
+  if (H.max_fac < 0 || H.max_fac > kMaxFac) return fail("factors per record");
+  if (H.len_f < 0 || H.len_j < 0 || H.len_f % 4 || H.len_j % 4) return fail("schedule lengths");
+  if (H.total_bytes < (int)sizeof(PlanHeader) || (size_t)H.total_bytes != size ||
+      H.total_bytes % 16)
+    return fail("table size");
+  const int64_t sf = (int64_t)H.len_f * kWarp, sj = (int64_t)H.len_j * kWarp;
+  auto region = [&](int32_t off, int64_t bytes_needed) {
+    return off >= (int32_t)sizeof(PlanHeader) && off % 16 == 0 &&
+           (int64_t)off + bytes_needed <= (int64_t)H.total_bytes;
+  };
+  if (!region(H.off_fd, sf * 16) || !region(H.off_ff, sf * 8) || !region(H.off_fm, sf * 8) ||
+      !region(H.off_jd, sj * 16) || !region(H.off_jf, sj * 8) || !region(H.off_jm, sj * 8) ||
+      !region(H.off_pre, (int64_t)H.n_pre * 8))
+    return fail("array offsets");
+  int64_t radix = 1;
+  for (int i = 0; i < H.n; ++i) {
+    if (H.deg[i] < 1 || H.deg[i] - 1 > H.maxexp || H.radix[i] != radix) return fail("degrees");
+    radix *= H.deg[i];
+  }
+  if (H.nstart != radix) return fail("path count");
+  // extended entries: level L may use plain entries and entries of levels < L
+  std::vector<char> ready(H.pw_total, 0);
+  std::fill(ready.begin(), ready.begin() + H.pw_size, 1);
+  if (H.level_off[0] != 0 || H.level_off[H.n_levels] != 2 * H.n_pre)
+    return fail("level ranges");
+  const uint32_t* pre = reinterpret_cast<const uint32_t*>(bytes + H.off_pre);
+  for (int L = 0; L < H.n_levels; ++L) {
+    const int w0 = H.level_off[L], w1 = H.level_off[L + 1];
+    if (w1 < w0 || (w1 - w0) % 2) return fail("level ranges");
+    for (int w = w0; w < w1; w += 2) {
+      const uint32_t t = pre[w], d = pre[w + 1];
+      for (int q = 0; q < 3; ++q) {
+        const uint32_t f = (t >> (10 * q)) & 0x3ffu;
+        if (f >= (uint32_t)H.pw_total || !ready[f]) return fail("extended entry factor");
+      }
+      if (d < (uint32_t)H.pw_size || d >= (uint32_t)H.pw_total) return fail("extended entry");
+    }
+    for (int w = w0; w < w1; w += 2) ready[pre[w + 1]] = 1;
+  }
+  for (int e = H.pw_size; e < H.pw_total; ++e)
+    if (!ready[e]) return fail("extended entry never computed");
+  // records: destinations inside the Jacobian rows, factors inside the
+  // computed table and within the kernel's schedule form, one finishing
+  // record per entry
+  auto check_schedule = [&](int len, int32_t off_m, const int32_t* cnt, bool jac) -> int {
+    const uint64_t* meta = reinterpret_cast<const uint64_t*>(bytes + off_m);
+    std::vector<char> finished((size_t)H.n * H.S, 0);
+    for (int l = 0; l < kWarp; ++l) {
+      if (cnt[l] < 0 || cnt[l] > len) return fail("records per lane");
+      for (int i = 0; i < len; ++i) {
+        const uint64_t m = meta[(size_t)i * kWarp + l];
+        if (i >= cnt[l]) {
+          if (m != 0) return fail("padding record");
+          continue;
+        }
+        const int dest = (int)(m & 0x3ff);
+        if (dest >= H.n * H.S || dest % H.S >= H.N) return fail("record destination");
+        for (int q = 0; q < kMaxFac; ++q) {
+          const int f = (int)((m >> (15 + 10 * q)) & 0x3ff);
+          if (f >= H.pw_total) return fail("record factor");
+          if (jac && q >= std::max(H.max_fac, 1) && f != 0) return fail("record schedule form");
+        }
+        if ((m >> 12) & kRecLast) {
+          if (finished[dest]) return fail("entry finished twice");
+          finished[dest] = 1;
+        }
+      }
+    }
+    return PHC_OK;
+  };
+  int st = check_schedule(H.len_f, H.off_fm, H.cnt_f, false);
+  if (st == PHC_OK) st = check_schedule(H.len_j, H.off_jm, H.cnt_j, true);
+  return st;
+}
+
 int validate_system(const phc_system* sys) {
   if (sys == nullptr) return PHC_ERR_INVALID_INPUT;
   const int n = sys->n;
@@ -330,7 +429,7 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   out->nstart = radix;
   out->nrec = nrec;
   out->max_fac = max_fac;
-  return PHC_OK;
+  return verify_plan(out->bytes.data(), out->bytes.size());
 }
 
 }  // namespace phc

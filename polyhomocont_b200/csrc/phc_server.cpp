@@ -20,6 +20,7 @@
 #include <memory>
 #include <mutex>
 #include <new>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -42,6 +43,9 @@ struct Request {
   int64_t npaths = 0;
   size_t dev_bytes = 0;
   int status = PHC_OK;
+  // why the request failed: error texts are per thread, so the engine's
+  // text travels with the request to the thread that asks for the result
+  std::string error;
   // results
   std::vector<phc_path_out> paths;
   std::vector<double> z, x, sols, realsols, ssols;
@@ -278,10 +282,11 @@ void engine_main(phc_server* S) {
       const bool kfin = (kq == cudaSuccess);
       if (kq != cudaSuccess && kq != cudaErrorNotReady) {
         // the batch kernel failed: its unfinished requests fail with it
-        set_last_error(cudaGetErrorString(kq));
+        set_last_error(std::string("batch kernel: ") + cudaGetErrorString(kq));
         for (auto& r : s.batch) {
           if (r->stage == 2) continue;
           r->status = PHC_ERR_CUDA;
+          r->error = last_error_text();
           r->t_done = Clock::now();
           r->done = true;
           r->stage = 2;
@@ -301,6 +306,7 @@ void engine_main(phc_server* S) {
             if (e != cudaSuccess) {
               cuda_fail(e, "server D2H");
               r.status = PHC_ERR_CUDA;
+              r.error = last_error_text();
               r.t_done = Clock::now();
               r.done = true;
               r.stage = 2;
@@ -355,6 +361,7 @@ void engine_main(phc_server* S) {
       if (st != PHC_OK) {
         for (auto& r : s.batch) {
           r->status = st;
+          r->error = last_error_text();
           r->t_done = Clock::now();
           r->done = true;
           S->completed++;
@@ -381,6 +388,7 @@ void engine_main(phc_server* S) {
   // abort what never started
   for (auto& r : S->pending) {
     r->status = PHC_ERR_ABORTED;
+    r->error = "the server stopped before the request started";
     r->done = true;
   }
   S->pending.clear();
@@ -562,7 +570,10 @@ int32_t phc_server_result(phc_server* S, uint64_t ticket, phc_solve_result* res,
   }
   if (latency_s)
     *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
-  if (r->status != PHC_OK) return r->status;
+  if (r->status != PHC_OK) {
+    set_last_error(r->error);
+    return r->status;
+  }
   const int n = r->n;
   res->counts = r->counts;
   if (res->paths) std::memcpy(res->paths, r->paths.data(), r->paths.size() * sizeof(phc_path_out));
