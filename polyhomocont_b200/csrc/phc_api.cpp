@@ -735,17 +735,24 @@ int32_t phc_solve_sparse(const phc_system* sys, const phc_solve_options* opts,
   st = validate_system(sys);
   if (st != PHC_OK) return st;
   HostHomotopy h;
-  st = homotopy_init(sys, so.seed, &h);  // gen%seed + hom%init
-  if (st != PHC_OK) return st;
-  if (!res->paths || !res->z || !res->x) return PHC_ERR_INVALID_INPUT;
-  const phc_homotopy hv = h.view();
   HostPlan hp;
-  st = build_plan(sys, &hv, &hp);
-  if (st != PHC_OK) return st;
-  st = run_paths_sync(hp, so, g, 1, h.nstart, res->paths, res->z, res->x);
-  if (st != PHC_OK) return st;
+  {
+    NvtxRange r("phc setup: homotopy and table compile");
+    st = homotopy_init(sys, so.seed, &h);  // gen%seed + hom%init
+    if (st != PHC_OK) return st;
+    if (!res->paths || !res->z || !res->x) return PHC_ERR_INVALID_INPUT;
+    const phc_homotopy hv = h.view();
+    st = build_plan(sys, &hv, &hp);
+    if (st != PHC_OK) return st;
+  }
+  {
+    NvtxRange r("phc track: copies and kernel");
+    st = run_paths_sync(hp, so, g, 1, h.nstart, res->paths, res->z, res->x);
+    if (st != PHC_OK) return st;
+  }
   res->counts.n = sys->n;
   res->counts.npaths = (int32_t)h.nstart;
+  NvtxRange r("phc bookkeeping");
   bookkeeping(sys->n, h.nstart, so, res->paths, res->x, res);
   return PHC_OK;
 }

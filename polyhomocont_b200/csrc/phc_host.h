@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <string>
@@ -82,6 +83,17 @@ inline int kernel_mode(int prec, int fac) {
 KOpts make_kopts(const phc_solve_options& so, const phc_gpu_options& g);
 phc_gpu_options gpu_defaults();
 phc_solve_options solve_defaults();
+
+// A named NVTX range over a host phase (table compile, tracking,
+// bookkeeping, sampling, tuning, serving batches), visible to profilers
+// that record NVTX (ncu --nvtx); without an attached tool it costs a
+// branch.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 void set_last_error(const std::string& s);
 // The calling thread's last error text (error texts are per thread).

@@ -40,6 +40,7 @@
 #include <map>
 #include <vector>
 
+#include "phc_host.h"
 #include "polyhomocont_b200.h"
 
 namespace {
@@ -187,6 +188,7 @@ struct Equation {
 extern "C" int32_t phc_sparse_sample(phc_sparse* s, int32_t n, const int32_t* degrees,
                                      phc_evaluator eval, void* ctx, int32_t seed,
                                      double* max_error) {
+  phc::NvtxRange range("phc sample user system");
   if (max_error) *max_error = 0.0;
   if (!s) return PHC_ERR_BAD_HANDLE;
   if (n < 1 || n >= 32 || !degrees || !eval) return PHC_ERR_INVALID_INPUT;

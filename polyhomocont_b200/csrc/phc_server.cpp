@@ -320,7 +320,10 @@ void engine_main(phc_server* S) {
           }
         }
         if (r.stage == 1 && cudaEventQuery(s.copied[i]) == cudaSuccess) {
-          finish_request(r, s.hbuf);
+          {
+            NvtxRange range("phc serve: finish request");
+            finish_request(r, s.hbuf);
+          }
           r.t_done = Clock::now();
           r.done = true;
           r.stage = 2;
@@ -357,7 +360,11 @@ void engine_main(phc_server* S) {
       }
       if (b.empty()) break;  // memory budget exhausted: wait for completions
       s.batch = b;
-      int st = launch_batch(S, s);
+      int st;
+      {
+        NvtxRange range("phc serve: launch batch");
+        st = launch_batch(S, s);
+      }
       if (st != PHC_OK) {
         for (auto& r : s.batch) {
           r->status = st;

@@ -50,6 +50,7 @@ using namespace phc;
 extern "C" int32_t phc_autotune(const phc_system* sys, const phc_solve_options* opts,
                                 phc_gpu_options* gpu, int64_t sample_paths,
                                 phc_tune_report* report) {
+  NvtxRange range("phc autotune");
   if (!gpu) return PHC_ERR_INVALID_INPUT;
   phc_gpu_options g = *gpu;
   const phc_solve_options so = opts ? *opts : solve_defaults();
