@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serving-systems", type=int, default=4096,
                     help="systems in the serving stream (0 skips the serving leg)")
+    ap.add_argument("--configs", action="store_true",
+                    help="instead of the benchmark line, measure the other single-system "
+                         "configurations (n=4 dense quadratic; n=4 singular cubic; n=16 with "
+                         "65536 paths): one JSON line each")
     ap.add_argument("--no-tune", action="store_true",
                     help="default launch configuration instead of the autotuner's "
                          "(for profiling: the timed launches then follow the warm-up directly)")
@@ -272,10 +276,105 @@ def serving(P, W, nsys, device, load=0.7, nslots=16, max_batch_systems=64,
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def run_configs(args):
+    """Mixed against plain FP64 on the other single-system configurations,
+    on one GPU: device-timed paths/s of both (each autotuned, L2 flushed
+    between timed launches), endpoint agreement and classification, and for
+    the singular cubic the error of the singular endpoints against the
+    exactly known root r. One JSON line per configuration."""
+    import torch
+    import polyhomocont_b200 as P
+    from polyhomocont_b200 import _abi
+    from polyhomocont_b200 import workloads as W
+    from polyhomocont_b200 import build as B
+
+    if not os.path.exists(_abi.LIB_PATH):
+        B.build()
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    n3, eqs3, r3 = W.singular_cubic()
+    cases = [
+        ("plain method: n=4, degrees 2, all 15 monomials of degree <= 2, 16 paths",
+         W.dense_quadratic(), None),
+        ("singular endpoints: n=4, degrees 3, (x_j - r_j)^2 and ^3 terms, 81 paths, "
+         "16 ending at the known root r", (n3, eqs3), r3),
+        ("large single system: n=16, degrees 2, 24 of 153 monomials per equation, "
+         "65536 paths", W.cfg5(), None),
+    ]
+    for name, (n, eqs), root in cases:
+        s = W.build(P.SparseSystem, n, eqs)
+        npaths = s.bezout()
+        arms = {}
+        for prec, key in ((P.PHC_PREC_MIXED, "mixed"), (P.PHC_PREC_FP64, "fp64")):
+            g, _ = P.autotune(s, gpu=P.default_gpu_options(prec))
+            plan = P.Plan(s, gpu=g)
+            out = torch.zeros(npaths * 96, dtype=torch.uint8, device=dev)
+            z = torch.zeros(npaths * (n + 1) * 2, dtype=torch.float64, device=dev)
+            for _ in range(max(args.warmup, 3)):
+                plan.launch(1, npaths, out.data_ptr(), z.data_ptr(), stream.cuda_stream)
+            torch.cuda.synchronize()
+            total = 0.0
+            for _ in range(args.steps):
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                plan.launch(1, npaths, out.data_ptr(), z.data_ptr(), stream.cuda_stream)
+                b.record(stream)
+                b.synchronize()
+                total += a.elapsed_time(b) * 1e-3
+            paths = np.frombuffer(out.cpu().numpy().tobytes(), dtype=P.PATH_DTYPE)
+            zz = z.cpu().numpy().view(np.complex128).reshape(npaths, n + 1)
+            arms[key] = {"paths_per_s": npaths * args.steps / total,
+                         "ms_per_launch": 1e3 * total / args.steps,
+                         "schedule": SCHED_NAMES[g.schedule],
+                         "warps_per_block": plan.config()["warps_per_block"],
+                         "paths": paths, "z": zz}
+            plan.close()
+        pm, pd = arms["mixed"]["paths"], arms["fp64"]["paths"]
+        same = all(np.array_equal(pm[k], pd[k]) for k in
+                   ("status", "winding_number", "at_infinity", "singular", "is_real"))
+        fin = (pd["status"] == 0) & (pd["at_infinity"] == 0) & (pd["singular"] == 0)
+        xm = arms["mixed"]["z"][:, :n] / arms["mixed"]["z"][:, n:n + 1]
+        xd = arms["fp64"]["z"][:, :n] / arms["fp64"]["z"][:, n:n + 1]
+        err = 0.0
+        if fin.any():
+            err = float(np.max(np.max(np.abs(xm[fin] - xd[fin]), axis=1) /
+                               np.maximum(1.0, np.max(np.abs(xd[fin]), axis=1))))
+        line = {"impl": "ours", "config": {"workload": name, "paths": npaths},
+                "metric": "paths/s, mixed vs plain FP64, device-timed, L2 flushed",
+                "steps": args.steps, "warmup": args.warmup,
+                "mixed": {k: v for k, v in arms["mixed"].items() if k not in ("paths", "z")},
+                "fp64": {k: v for k, v in arms["fp64"].items() if k not in ("paths", "z")},
+                "mixed_vs_fp64": arms["mixed"]["paths_per_s"] / arms["fp64"]["paths_per_s"],
+                "classification_identical": bool(same),
+                "regular_endpoint_max_rel_err_mixed_vs_fp64": err,
+                "counts": {"regular": int(fin.sum()),
+                           "singular": int(((pd["status"] == 0) & (pd["singular"] != 0)
+                                            & (pd["at_infinity"] == 0)).sum()),
+                           "infinite": int(((pd["status"] == 0) & (pd["at_infinity"] != 0)).sum()),
+                           "failed": int((pd["status"] != 0).sum())}}
+        if root is not None:
+            def root_err(p, x):
+                sing = (p["status"] == 0) & (p["singular"] != 0) & (p["at_infinity"] == 0)
+                if not sing.any():
+                    return None
+                return float(np.max(np.max(np.abs(x[sing] - root[None, :]), axis=1)) /
+                             max(1.0, float(np.max(np.abs(root)))))
+            line["singular_endpoint_err_vs_exact_root"] = {"mixed": root_err(pm, xm),
+                                                           "fp64": root_err(pd, xd)}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.configs:
+        run_configs(args)
         return
     rank, world, local = dist_env()
     import torch
