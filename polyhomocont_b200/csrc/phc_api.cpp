@@ -389,17 +389,17 @@ static double norm_inf_c(const double* v, int n) {
 // reference.
 class PointSet {
  public:
-  PointSet(int n, double tol, int64_t expect)
-      : n_(n), tol_(tol), width_(64.0 * tol) {
+  // Points are rows of the caller's array x ([npaths][n] complex); the set
+  // stores row indices, not copies.
+  PointSet(int n, double tol, const double* x, int64_t expect)
+      : n_(n), tol_(tol), width_(64.0 * tol), x_(x) {
     size_t cap = 64;
     while (cap < 2 * (size_t)std::max<int64_t>(expect, 1)) cap <<= 1;
     keys_.assign(cap, 0);
     heads_.assign(cap, -1);
-    pts_.reserve((size_t)std::max<int64_t>(expect, 1) * 2 * n);
-    next_.reserve((size_t)std::max<int64_t>(expect, 1));
   }
-  int size() const { return (int)next_.size(); }
-  const std::vector<double>& data() const { return pts_; }
+  int size() const { return (int)rows_.size(); }
+  const double* point(int j) const { return x_ + (size_t)rows_[j] * 2 * n_; }
 
   int find(const double* x) const {
     const double scale = std::max(1.0, norm_inf_c(x, n_));
@@ -424,11 +424,13 @@ class PointSet {
     return best < 0 ? 0 : best + 1;
   }
 
-  void add(const double* x) {
+  // adds row k of x (the point x + k*2n)
+  void add(int64_t k) {
     const int j = size();
-    pts_.insert(pts_.end(), x, x + 2 * (size_t)n_);
-    if (std::isfinite(x[0]) && width_ > 0.0 && std::fabs(x[0]) <= 1e15 * width_) {
-      const long long b = bucket(x[0]);
+    rows_.push_back(k);
+    const double x0 = point(j)[0];
+    if (std::isfinite(x0) && width_ > 0.0 && std::fabs(x0) <= 1e15 * width_) {
+      const long long b = bucket(x0);
       size_t slot = probe(b);
       if (heads_[slot] < 0) {
         keys_[slot] = b;
@@ -475,7 +477,7 @@ class PointSet {
   }
   // max_i |x_i - p_i| <= rho, decided on squares away from the threshold
   bool within(const double* x, int j, double rho) const {
-    const double* p = pts_.data() + (size_t)j * 2 * n_;
+    const double* p = point(j);
     const double r2 = rho * rho;
     bool exact = !(r2 >= kSqLo && r2 <= kSqHi);
     double m2 = 0.0;
@@ -496,7 +498,8 @@ class PointSet {
   }
   int n_;
   double tol_, width_;
-  std::vector<double> pts_;
+  const double* x_;
+  std::vector<int64_t> rows_;     // row of x of each stored point
   std::vector<int> next_;         // previous point in the same bucket, or -1
   std::vector<long long> keys_;   // open-addressing table: bucket -> newest point
   std::vector<int> heads_;
@@ -507,7 +510,7 @@ class PointSet {
 void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out* paths,
                  const double* x, phc_solve_result* res) {
   phc_solve_counts& c = res->counts;
-  PointSet sols(n, o.dedup_tol, npaths), ssols(n, o.singular_dedup_tol, npaths);
+  PointSet sols(n, o.dedup_tol, x, npaths), ssols(n, o.singular_dedup_tol, x, 64);
   std::vector<int> mult;
   for (int64_t k = 0; k < npaths; ++k) {
     phc_path_out& p = paths[k];
@@ -523,7 +526,7 @@ void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out
       if (j > 0) {
         mult[j - 1]++;
       } else {
-        ssols.add(xk);
+        ssols.add(k);
         mult.push_back(1);
         j = ssols.size();
       }
@@ -533,7 +536,7 @@ void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out
       if (j > 0) {
         c.nduplicates++;
       } else {
-        sols.add(xk);
+        sols.add(k);
         j = sols.size();
       }
       p.solution_index = j;
@@ -542,16 +545,18 @@ void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out
   const int nsol = sols.size(), nsing = ssols.size();
   c.nsolutions = nsol;
   c.nsingular = nsing;
-  if (res->solutions && nsol)
-    std::memcpy(res->solutions, sols.data().data(), sols.data().size() * sizeof(double));
-  if (res->singular_solutions && nsing)
-    std::memcpy(res->singular_solutions, ssols.data().data(), ssols.data().size() * sizeof(double));
+  const size_t row = (size_t)2 * n * sizeof(double);
+  if (res->solutions)
+    for (int j = 0; j < nsol; ++j) std::memcpy(res->solutions + (size_t)j * 2 * n, sols.point(j), row);
+  if (res->singular_solutions)
+    for (int j = 0; j < nsing; ++j)
+      std::memcpy(res->singular_solutions + (size_t)j * 2 * n, ssols.point(j), row);
   if (res->multiplicities)
     for (int j = 0; j < nsing; ++j) res->multiplicities[j] = mult[j];
   // collect_real, src/solve.f90:402-426
   int nreal = 0;
   for (int j = 0; j < nsol; ++j) {
-    const double* sj = sols.data().data() + (size_t)j * 2 * n;
+    const double* sj = sols.point(j);
     double imax = 0.0;
     for (int i = 0; i < n; ++i) imax = std::max(imax, std::fabs(sj[2 * i + 1]));
     if (imax <= o.real_tol * std::max(1.0, norm_inf_c(sj, n))) {
