@@ -57,6 +57,12 @@ def parse():
                     help="instead of the benchmark line, measure the other single-system "
                          "configurations (n=4 dense quadratic; n=4 singular cubic; n=16 with "
                          "65536 paths): one JSON line each")
+    ap.add_argument("--config-filter", default="",
+                    help="with --configs: only the configurations whose description "
+                         "contains this text")
+    ap.add_argument("--max-paths", type=int, default=0,
+                    help="with --configs: track only the first N paths of each system "
+                         "(a small case for profiler captures; the line says so)")
     ap.add_argument("--no-tune", action="store_true",
                     help="default launch configuration instead of the autotuner's "
                          "(for profiling: the timed launches then follow the warm-up directly)")
@@ -304,11 +310,18 @@ def run_configs(args):
          "65536 paths", W.cfg5(), None),
     ]
     for name, (n, eqs), root in cases:
+        if args.config_filter and args.config_filter not in name:
+            continue
         s = W.build(P.SparseSystem, n, eqs)
         npaths = s.bezout()
+        if args.max_paths > 0:
+            npaths = min(npaths, args.max_paths)
         arms = {}
         for prec, key in ((P.PHC_PREC_MIXED, "mixed"), (P.PHC_PREC_FP64, "fp64")):
-            g, _ = P.autotune(s, gpu=P.default_gpu_options(prec))
+            if args.no_tune:
+                g = P.default_gpu_options(prec)
+            else:
+                g, _ = P.autotune(s, gpu=P.default_gpu_options(prec))
             plan = P.Plan(s, gpu=g)
             out = torch.zeros(npaths * 96, dtype=torch.uint8, device=dev)
             z = torch.zeros(npaths * (n + 1) * 2, dtype=torch.float64, device=dev)
@@ -343,7 +356,9 @@ def run_configs(args):
         if fin.any():
             err = float(np.max(np.max(np.abs(xm[fin] - xd[fin]), axis=1) /
                                np.maximum(1.0, np.max(np.abs(xd[fin]), axis=1))))
-        line = {"impl": "ours", "config": {"workload": name, "paths": npaths},
+        line = {"impl": "ours", "config": {"workload": name, "paths": npaths,
+                                           "paths_of_system": s.bezout(),
+                                           "tuned": not args.no_tune},
                 "metric": "paths/s, mixed vs plain FP64, device-timed, L2 flushed",
                 "steps": args.steps, "warmup": args.warmup,
                 "mixed": {k: v for k, v in arms["mixed"].items() if k not in ("paths", "z")},
