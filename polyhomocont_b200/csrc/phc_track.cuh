@@ -39,16 +39,17 @@ struct UnitRes {
 constexpr int kCondChunk = 4;
 
 // One unit: an evaluation of H, H_z and H_t followed by one elimination.
-// prec selects the arithmetic (only the FP64 form exists when MIXED is
-// false):
-//   0: FP64 evaluation and elimination (FP64 tracker, FP64 retries, the
-//      end game's backward errors, refine, cond1)
-//   1: FP32 evaluation and elimination (mixed predictor, tangent)
-//   2: FP64 evaluation, FP32 elimination (mixed corrector: the residual in
-//      FP64, the update in FP32)
-// Every piece of code -- the FP32 and FP64 evaluation, the FP32 and FP64
-// elimination -- appears once in the kernel, which keeps the instruction
-// footprint of the mixed kernel close to that of the FP64 kernel.
+// The evaluation is always FP64; prec selects the elimination (only the
+// FP64 form exists when MIXED is false):
+//   0: FP64 elimination (FP64 tracker, FP64 retries, the end game's
+//      backward errors, refine, cond1)
+//   1: FP32 elimination (mixed predictor and corrector: H, H_z, H_t and the
+//      residual in FP64, the tangent and the Newton update in FP32)
+// An FP32 evaluation for the predictor was measured and dropped: it saved
+// less than the extra code cost in instruction-cache misses (the mixed
+// kernel for 17 unknowns was 4 % slower with it, the one for 11 unknowns 2 %).
+// Every piece of code -- the evaluation, the FP32 and the FP64 elimination
+// -- appears once in the kernel.
 // UK_COND eliminates against the unit vectors e_c0 .. e_c0+3 (cond1,
 // src/linalg.f90:135-174); the state machine runs one such unit per chunk.
 // Rows of up to 16 columns use the split layout (two lanes per row, half
@@ -93,71 +94,65 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
   const int row = lane & (L::kRows - 1);
   const bool owner = lane < L::kRows;
   cd h, ht;
-  cpx<float> as[RW];
-  if (!MIXED || prec != 1) {
-    cpx<double> a[RW];
-    evaluate_rows<NM, double, F>(C, ws, zin, t, lane, a, h, ht);
-    if (kind == UK_BACKERR) {
-      // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
-      // absolute row sum of H_z
-      double rs = 0.0;
+  cpx<double> a[RW];
+  evaluate_rows<NM, double, F>(C, ws, zin, t, lane, a, h, ht);
+  if (kind == UK_BACKERR) {
+    // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
+    // absolute row sum of H_z
+    double rs = 0.0;
 #pragma unroll
-      for (int j = 0; j < RW; ++j) rs += cabs(a[j]);
-      rs = row_sum<L::kLanes>(rs);
-      u.a1 = warp_max_nonneg(row < N ? cabs(h) : 0.0);
-      u.a2 = warp_max_nonneg(row < N ? rs : 0.0);
-      u.ok = true;
-      return;
-    }
-    if (kind == UK_COND) {
-      u.h = h;
-      if (c0 == 0) {
-        double anorm = 0.0;
-#pragma unroll
-        for (int j = 0; j < RW; ++j) {
-          if constexpr (L::kSplit)
-            anorm = fmax(anorm, part_sum<L::kLanes>(row < N ? cabs(a[j]) : 0.0));
-          else if (j < N)
-            anorm = fmax(anorm, warp_sum(row < N ? cabs(a[j]) : 0.0));
-        }
-        if constexpr (L::kSplit) anorm = warp_max_nonneg(anorm);
-        u.a1 = anorm;
-      }
-      cd r[kCondChunk];
-#pragma unroll
-      for (int q = 0; q < kCondChunk; ++q)
-        r[q] = (row == c0 + q) ? cone<double>() : czero<double>();
-      if (!eliminate<NM, kCondChunk, double>(a, r, N, lane, ws.piv)) {
-        u.ok = false;  // cond1 of an exactly singular matrix
-        return;
-      }
-      double ainv = 0.0;
-#pragma unroll
-      for (int q = 0; q < kCondChunk; ++q) {
-        if (c0 + q < N) ainv = fmax(ainv, warp_sum(owner && row < N ? cabs(r[q]) : 0.0));
-      }
-      u.a2 = ainv;
-      u.ok = true;
-      return;
-    }
-    if (!MIXED || prec == 0) {
-      cd r[1];
-      r[0] = (kind == UK_TANGENT) ? -(ht * dt) : -h;
-      u.ok = eliminate<NM, 1, double>(a, r, N, lane, ws.piv);
-      if (!u.ok) return;
-      const cd x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
-      u.x = (lane < N) ? x : czero<double>();
-      return;
-    }
-    // mixed corrector: FP64 residual, FP32 update
-    if constexpr (MIXED) {
-#pragma unroll
-      for (int j = 0; j < RW; ++j) as[j] = ccast<float>(a[j]);
-    }
-  } else {
-    evaluate_rows<NM, float, F>(C, ws, zin, t, lane, as, h, ht);
+    for (int j = 0; j < RW; ++j) rs += cabs(a[j]);
+    rs = row_sum<L::kLanes>(rs);
+    u.a1 = warp_max_nonneg(row < N ? cabs(h) : 0.0);
+    u.a2 = warp_max_nonneg(row < N ? rs : 0.0);
+    u.ok = true;
+    return;
   }
+  if (kind == UK_COND) {
+    u.h = h;
+    if (c0 == 0) {
+      double anorm = 0.0;
+#pragma unroll
+      for (int j = 0; j < RW; ++j) {
+        if constexpr (L::kSplit)
+          anorm = fmax(anorm, part_sum<L::kLanes>(row < N ? cabs(a[j]) : 0.0));
+        else if (j < N)
+          anorm = fmax(anorm, warp_sum(row < N ? cabs(a[j]) : 0.0));
+      }
+      if constexpr (L::kSplit) anorm = warp_max_nonneg(anorm);
+      u.a1 = anorm;
+    }
+    cd r[kCondChunk];
+#pragma unroll
+    for (int q = 0; q < kCondChunk; ++q)
+      r[q] = (row == c0 + q) ? cone<double>() : czero<double>();
+    if (!eliminate<NM, kCondChunk, double>(a, r, N, lane, ws.piv)) {
+      u.ok = false;  // cond1 of an exactly singular matrix
+      return;
+    }
+    double ainv = 0.0;
+#pragma unroll
+    for (int q = 0; q < kCondChunk; ++q) {
+      if (c0 + q < N) ainv = fmax(ainv, warp_sum(owner && row < N ? cabs(r[q]) : 0.0));
+    }
+    u.a2 = ainv;
+    u.ok = true;
+    return;
+  }
+  if (!MIXED || prec == 0) {
+    cd r[1];
+    r[0] = (kind == UK_TANGENT) ? -(ht * dt) : -h;
+    u.ok = eliminate<NM, 1, double>(a, r, N, lane, ws.piv);
+    if (!u.ok) return;
+    const cd x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
+    u.x = (lane < N) ? x : czero<double>();
+    return;
+  }
+  // mixed predictor and corrector: FP64 evaluation, FP32 elimination
   if constexpr (MIXED) {
+    cpx<float> as[RW];
+#pragma unroll
+    for (int j = 0; j < RW; ++j) as[j] = ccast<float>(a[j]);
     cpx<float> r[1];
     r[0] = ccast<float>((kind == UK_TANGENT) ? -(ht * dt) : -h);
     u.ok = eliminate<NM, 1, float>(as, r, N, lane, ws.piv);
@@ -275,7 +270,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
   bool att64 = true;
   // pending unit
   int uk = UK_TANGENT, pc_after = PC_FINISH;
-  int u_prec = 0;  // 0: FP64, 1: FP32 evaluation + elimination, 2: FP64 evaluation + FP32 elimination
+  int u_prec = 0;  // 0: FP64 elimination, 1: FP32 elimination (the evaluation is FP64)
   cd tin = z, dtin = z;
   UnitRes U;
   U.x = U.h = czero<double>();
@@ -407,7 +402,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
                 stage = 4;
                 dnorm_prev = kHuge;
                 uk = UK_NEWTON;
-                u_prec = att64 ? 0 : 2;
+                u_prec = att64 ? 0 : 1;
                 zin = zp;
                 if (sn != s + ds) tin = seg_t(st, sn);  // else t(s + ds) of stage 3
               }

@@ -14,10 +14,10 @@ largest homogenized exponent of unknown j:
 
 A path's flops follow from its unit counters (phc_path_out): predictor,
 corrector and refine units cost F_unit, evaluation-only units F_eval + F_hom,
-a cond1 call F_LU + N F_sol. In mixed precision a corrector unit evaluates
-the residual in FP64 (F_res64 = sum_k (6 s_k + 2) + sum_i (12 d_i + 46) + 8 N)
-and everything else of a predictor/corrector unit in FP32, unless the unit
-ran in FP64 (counter n_fp64_retry).
+a cond1 call F_LU + N F_sol. In mixed precision a predictor or corrector
+unit evaluates H, H_z and H_t in FP64 (F_eval + F_hom) and eliminates in
+FP32 (F_LU + F_sol), unless the whole unit ran in FP64 (counter
+n_fp64_retry).
 """
 import numpy as np
 
@@ -32,9 +32,8 @@ def unit_model(n, deg, hexps):
     f_hom = float(6 * n * N + np.sum(12 * deg + 46) + 8 * N)
     f_lu = float(sum(8 * r * r + 9 * r + 11 for r in range(1, N)) + 3 * N)
     f_sol = float(8 * N * (N - 1) + 6 * N)
-    f_res64 = float(np.sum(6 * s + 2) + np.sum(12 * deg + 46) + 8 * N)
     return dict(F_eval=f_eval, F_hom=f_hom, F_LU=f_lu, F_sol=f_sol,
-                F_unit=f_eval + f_hom + f_lu + f_sol, F_res64=f_res64, N=N)
+                F_unit=f_eval + f_hom + f_lu + f_sol, N=N)
 
 
 def path_flops(model, paths, mixed):
@@ -50,8 +49,6 @@ def path_flops(model, paths, mixed):
         return (t + c) * M["F_unit"] + other64, 0.0
     u64 = paths["n_fp64_retry"].astype(np.float64).sum()
     u32 = max(t + c - u64, 0.0)
-    newton_frac = c / max(t + c, 1.0)
-    c32 = u32 * newton_frac
-    f64 = other64 + u64 * M["F_unit"] + c32 * M["F_res64"]
-    f32 = u32 * M["F_unit"] - c32 * M["F_res64"]
+    f64 = other64 + u64 * M["F_unit"] + u32 * (M["F_eval"] + M["F_hom"])
+    f32 = u32 * (M["F_LU"] + M["F_sol"])
     return f64, f32
