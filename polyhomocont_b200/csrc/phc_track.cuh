@@ -922,12 +922,10 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
 template <int PREC>
 __device__ __forceinline__ WarpWS warp_workspace(const PlanHeader& P, unsigned char* wbase,
                                                 WarpState** st) {
-  const WsLayout L = ws_layout(P.n, P.S, P.pw_total, PREC == PHC_PREC_MIXED);
+  const WsLayout L = ws_layout(P.n, P.S, P.pw_total);
   WarpWS ws;
   ws.pwd = reinterpret_cast<cd*>(wbase + L.pwd);
-  ws.pwf = reinterpret_cast<cf*>(wbase + L.pwf);
   ws.jd = reinterpret_cast<cd*>(wbase + L.jd);
-  ws.jf = reinterpret_cast<cf*>(wbase + L.jf);
   ws.piv = reinterpret_cast<int*>(wbase + L.piv);
   *st = reinterpret_cast<WarpState*>(wbase + L.st);
   return ws;
@@ -944,7 +942,6 @@ __device__ __forceinline__ void init_jacobian_buffer(const PlanHeader& P, const 
     cd v = czero<double>();
     if (row == P.n && col < P.N) v = mkc<double>(P.patch[col][0], P.patch[col][1]);
     sts(&ws.jd[q], v);
-    if (PREC == PHC_PREC_MIXED) sts(&ws.jf[q], ccast<float>(v));
   }
   __syncwarp();
 }
