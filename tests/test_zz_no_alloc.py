@@ -74,7 +74,7 @@ def test_noalloc_rejects_oversize_table():
     import torch
     if not torch.cuda.is_available():
         pytest.fail("GPU test needs a CUDA device")
-    n = 20
+    n = 24  # all 325 monomials of degree <= 2 per equation: a 359 KiB table
     sys = P.SparseSystem(n)
     mons = W.monomials(n, 2)
     for i in range(n):
