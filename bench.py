@@ -227,7 +227,7 @@ class ClockSampler:
 # `python bench.py --steps 2 --warmup 3 --no-e2e --no-cpu --serving-systems 0`
 # (profiles/track_kernel_n10_1024paths.md). The kernel is compute- and
 # latency-bound; its traffic is the table, the start data and the results.
-NCU_DRAM_BYTES_PER_LAUNCH = 131584
+NCU_DRAM_BYTES_PER_LAUNCH = 123904
 SCHED_NAMES = {0: "grid", 1: "persistent"}
 
 
