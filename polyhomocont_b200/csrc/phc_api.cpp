@@ -211,7 +211,7 @@ int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, Lau
   int tw = 4, tc = 1;
   tuned_launch(device, cfg->precision, cfg->persistent, cfg->nm, &tw, &tc);
   cfg->chunk = g.chunk > 0 ? g.chunk : tc;
-  cfg->ws_bytes = ws_layout(hp.n, hp.S, hp.pw_size).bytes;
+  cfg->ws_bytes = ws_layout(hp.n, hp.S, hp.pw_size, cfg->precision == PHC_PREC_MIXED).bytes;
   const int plan_bytes = align16((int)hp.bytes.size());
   const int smax = device_smem_optin(device);
   int warps = g.warps_per_block > 0 ? g.warps_per_block : tw;

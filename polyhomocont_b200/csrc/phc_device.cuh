@@ -285,15 +285,19 @@ __device__ __forceinline__ int warp_argmax_first(float key, bool cand, float& km
 
 // ---- per-warp workspace -------------------------------------------------------
 struct WarpWS {
-  cd* pwd;    // power table z_j^e
+  cd* pwd;    // power table z_j^e, FP64
+  cf* pwf;    // power table, FP32 (mixed precision only)
   cd* jd;     // Jacobian of F^h, row-major, stride S
+  cf* jf;
   int* piv;   // pivot row (lane) of each column
 };
 
 template <typename T> __device__ __forceinline__ cpx<T>* ws_pw(const WarpWS& w);
 template <> __device__ __forceinline__ cd* ws_pw<double>(const WarpWS& w) { return w.pwd; }
+template <> __device__ __forceinline__ cf* ws_pw<float>(const WarpWS& w) { return w.pwf; }
 template <typename T> __device__ __forceinline__ cpx<T>* ws_j(const WarpWS& w);
 template <> __device__ __forceinline__ cd* ws_j<double>(const WarpWS& w) { return w.jd; }
+template <> __device__ __forceinline__ cf* ws_j<float>(const WarpWS& w) { return w.jf; }
 
 // Constants of the system held in registers for the lifetime of a warp. The
 // shared-memory table could alias the workspace that the evaluation writes,
@@ -310,6 +314,7 @@ struct WarpConst {
   cd b;             // b_lane
   cd gamma;
   const cd* coefd;  // Jacobian schedule arrays (shared memory)
+  const cf* coeff;
   const uint2* meta;
   const double (*patch)[2];
 };
@@ -331,6 +336,7 @@ __device__ __forceinline__ WarpConst load_warp_const(const PlanHeader& P,
   C.b = lane < P.n ? mkc<double>(P.b[lane][0], P.b[lane][1]) : czero<double>();
   C.gamma = mkc<double>(P.gamma[0], P.gamma[1]);
   C.coefd = reinterpret_cast<const cd*>(pb + P.off_jd);
+  C.coeff = reinterpret_cast<const cf*>(pb + P.off_jf);
   C.meta = reinterpret_cast<const uint2*>(pb + P.off_jm);
   C.patch = P.patch;
   return C;
@@ -339,6 +345,9 @@ __device__ __forceinline__ WarpConst load_warp_const(const PlanHeader& P,
 template <typename T> __device__ __forceinline__ const cpx<T>* wc_coef(const WarpConst& C);
 template <> __device__ __forceinline__ const cd* wc_coef<double>(const WarpConst& C) {
   return C.coefd;
+}
+template <> __device__ __forceinline__ const cf* wc_coef<float>(const WarpConst& C) {
+  return C.coeff;
 }
 
 // ---- sparse evaluation ----------------------------------------------------

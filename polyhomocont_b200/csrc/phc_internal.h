@@ -45,10 +45,9 @@ enum : unsigned {
 constexpr int kMaxLevels = 8;
 
 // Records are stored lane-interleaved: record i of lane l sits in slot
-// i * 32 + l of two arrays (FP64 coefficient, metadata), so the 32 lanes of
-// a warp read consecutive 16- and 8-byte words without shared-memory bank
-// conflicts. (The evaluation is FP64 in both precision modes, so the table
-// carries no FP32 coefficients.)
+// i * 32 + l of three arrays (FP64 coefficient, FP32 coefficient, metadata),
+// so the 32 lanes of a warp read consecutive 16-, 8- and 8-byte words
+// without shared-memory bank conflicts.
 struct alignas(16) PlanHeader {
   int32_t n;            // variables / equations
   int32_t N;            // unknowns n + 1
@@ -58,8 +57,8 @@ struct alignas(16) PlanHeader {
   int32_t len_f;        // slots per lane of the f schedule
   int32_t len_j;        // slots per lane of the Jacobian schedule
   int32_t total_bytes;  // header + arrays (multiple of 16)
-  int32_t off_fd, off_fm;  // byte offsets of the f schedule arrays
-  int32_t off_jd, off_jm;  // byte offsets of the Jacobian schedule arrays
+  int32_t off_fd, off_ff, off_fm;  // byte offsets of the f schedule arrays
+  int32_t off_jd, off_jf, off_jm;  // byte offsets of the Jacobian schedule arrays
   int32_t nrec;         // records of both schedules
   int32_t n_pre;        // extended power-table entries (products of three)
   int32_t off_pre;      // byte offset of their packed factor triples (uint32)
@@ -175,18 +174,18 @@ struct alignas(16) WarpState {
 // Per-warp shared-memory workspace layout (byte offsets from the warp's
 // base), shared by host (sizing) and device (addressing).
 struct WsLayout {
-  int pwd, jd, piv, st, bytes;
+  int pwd, pwf, jd, jf, piv, st, bytes;
 };
 
 PHC_HD inline int align16(int x) { return (x + 15) & ~15; }
 
-// The evaluation is FP64 in both precision modes, so the layout is the same
-// for both.
-PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size) {
+PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size, bool mixed) {
   WsLayout L;
   int off = 0;
   L.pwd = off; off += align16(pw_size * 16);
+  L.pwf = off; off += mixed ? align16(pw_size * 8) : 0;
   L.jd = off; off += align16((n + 1) * S * 16);  // rows 0..n-1: dF^h, row n: patch
+  L.jf = off; off += mixed ? align16((n + 1) * S * 8) : 0;
   L.piv = off; off += kWarp * 4;
   L.st = off; off += align16((int)sizeof(WarpState));
   L.bytes = off;

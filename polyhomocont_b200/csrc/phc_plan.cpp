@@ -145,8 +145,9 @@ void schedule(const std::vector<std::vector<Contribution>>& entries,
 
 // Writes one schedule's lane-interleaved arrays at the given offsets.
 void store_schedule(const std::vector<std::vector<PackedRec>>& lanes, int len,
-                    unsigned char* base, int off_d, int off_m, int32_t* cnt) {
+                    unsigned char* base, int off_d, int off_f, int off_m, int32_t* cnt) {
   double* cd = reinterpret_cast<double*>(base + off_d);
+  float* cf = reinterpret_cast<float*>(base + off_f);
   uint64_t* cm = reinterpret_cast<uint64_t*>(base + off_m);
   for (int l = 0; l < kWarp; ++l) {
     cnt[l] = (int32_t)lanes[l].size();
@@ -156,6 +157,8 @@ void store_schedule(const std::vector<std::vector<PackedRec>>& lanes, int len,
       if (i < (int)lanes[l].size()) r = lanes[l][i];
       cd[2 * slot] = r.cre;
       cd[2 * slot + 1] = r.cim;
+      cf[2 * slot] = (float)r.cre;
+      cf[2 * slot + 1] = (float)r.cim;
       cm[slot] = r.meta;
     }
   }
@@ -202,8 +205,8 @@ int verify_plan(const unsigned char* bytes, size_t size) {
     return off >= (int32_t)sizeof(PlanHeader) && off % 16 == 0 &&
            (int64_t)off + bytes_needed <= (int64_t)H.total_bytes;
   };
-  if (!region(H.off_fd, sf * 16) || !region(H.off_fm, sf * 8) || !region(H.off_jd, sj * 16) ||
-      !region(H.off_jm, sj * 8) ||
+  if (!region(H.off_fd, sf * 16) || !region(H.off_ff, sf * 8) || !region(H.off_fm, sf * 8) ||
+      !region(H.off_jd, sj * 16) || !region(H.off_jf, sj * 8) || !region(H.off_jm, sj * 8) ||
       !region(H.off_pre, (int64_t)H.n_pre * 8))
     return fail("array offsets");
   int64_t radix = 1;
@@ -401,8 +404,10 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   };
   const size_t sf = (size_t)len_f * kWarp, sj = (size_t)len_j * kWarp;
   H.off_fd = take(sf * 16);
+  H.off_ff = take(sf * 8);
   H.off_fm = take(sf * 8);
   H.off_jd = take(sj * 16);
+  H.off_jf = take(sj * 8);
   H.off_jm = take(sj * 8);
   H.off_pre = take(pre_packed.size() * 4);
   H.total_bytes = (int32_t)off;
@@ -411,8 +416,8 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   for (const auto& v : lj) nrec += (int)v.size();
   H.nrec = nrec;
   out->bytes.assign(off, 0);
-  store_schedule(lf, len_f, out->bytes.data(), H.off_fd, H.off_fm, H.cnt_f);
-  store_schedule(lj, len_j, out->bytes.data(), H.off_jd, H.off_jm, H.cnt_j);
+  store_schedule(lf, len_f, out->bytes.data(), H.off_fd, H.off_ff, H.off_fm, H.cnt_f);
+  store_schedule(lj, len_j, out->bytes.data(), H.off_jd, H.off_jf, H.off_jm, H.cnt_j);
   if (!pre_packed.empty())
     std::memcpy(out->bytes.data() + H.off_pre, pre_packed.data(), pre_packed.size() * 4);
   std::memcpy(out->bytes.data(), &H, sizeof(H));

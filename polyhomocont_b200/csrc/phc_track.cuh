@@ -39,17 +39,24 @@ struct UnitRes {
 constexpr int kCondChunk = 4;
 
 // One unit: an evaluation of H, H_z and H_t followed by one elimination.
-// The evaluation is always FP64; prec selects the elimination (only the
-// FP64 form exists when MIXED is false):
-//   0: FP64 elimination (FP64 tracker, FP64 retries, the end game's
-//      backward errors, refine, cond1)
-//   1: FP32 elimination (mixed predictor and corrector: H, H_z, H_t and the
-//      residual in FP64, the tangent and the Newton update in FP32)
-// An FP32 evaluation for the predictor was measured and dropped: it saved
-// less than the extra code cost in instruction-cache misses (the mixed
-// kernel for 17 unknowns was 4 % slower with it, the one for 11 unknowns 2 %).
-// Every piece of code -- the evaluation, the FP32 and the FP64 elimination
-// -- appears once in the kernel.
+// prec selects the arithmetic (only the FP64 form exists when MIXED is
+// false):
+//   0: FP64 evaluation and elimination (FP64 tracker, FP64 retries, the
+//      end game's backward errors, refine, cond1)
+//   1: FP64 evaluation, FP32 elimination (mixed corrector: the residual in
+//      FP64, the update in FP32; mixed predictor unless EVAL32)
+//   2: FP32 evaluation and elimination (mixed predictor when EVAL32)
+// EVAL32 compiles the FP32 evaluation into the kernel. It pays where one
+// path's latency sets the time and the kernel is small: the single-system
+// kernels for rows of up to 8 columns (n <= 7), whose paths run nearly
+// alone. Elsewhere the second evaluation body costs more in instruction
+// fetch than it saves: the batch kernels, throughput-bound, and the wider
+// rows, whose bodies are long. Measured on one B200: n=4 systems 1.00 ms
+// with an FP64 evaluation against 0.85 ms with an FP32 one; 17 unknowns,
+// 65,536 paths, 342.6 ms against 358.3 ms; the serving stream's capacity
+// about 2,200 against 1,800 systems/s.
+// Every piece of code -- each evaluation, the FP32 and the FP64
+// elimination -- appears once in the kernel.
 // UK_COND eliminates against the unit vectors e_c0 .. e_c0+3 (cond1,
 // src/linalg.f90:135-174); the state machine runs one such unit per chunk.
 // Rows of up to 16 columns use the split layout (two lanes per row, half
@@ -84,7 +91,7 @@ __device__ __forceinline__ bool eliminate(cpx<T> (&a)[RowLayout<NM>::kRegs], cpx
     return gauss_jordan<NM, R, T>(a, r, N, lane, piv);
 }
 
-template <int NM, bool MIXED, int F>
+template <int NM, bool MIXED, bool EVAL32, int F>
 __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, int kind, int prec,
                                          int c0, cd zin, cd t, cd dt, int lane, UnitRes& u) {
   using L = RowLayout<NM>;
@@ -94,65 +101,71 @@ __device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, i
   const int row = lane & (L::kRows - 1);
   const bool owner = lane < L::kRows;
   cd h, ht;
-  cpx<double> a[RW];
-  evaluate_rows<NM, double, F>(C, ws, zin, t, lane, a, h, ht);
-  if (kind == UK_BACKERR) {
-    // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
-    // absolute row sum of H_z
-    double rs = 0.0;
+  cpx<float> as[RW];
+  if (!MIXED || !EVAL32 || prec != 2) {
+    cpx<double> a[RW];
+    evaluate_rows<NM, double, F>(C, ws, zin, t, lane, a, h, ht);
+    if (kind == UK_BACKERR) {
+      // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
+      // absolute row sum of H_z
+      double rs = 0.0;
 #pragma unroll
-    for (int j = 0; j < RW; ++j) rs += cabs(a[j]);
-    rs = row_sum<L::kLanes>(rs);
-    u.a1 = warp_max_nonneg(row < N ? cabs(h) : 0.0);
-    u.a2 = warp_max_nonneg(row < N ? rs : 0.0);
-    u.ok = true;
-    return;
-  }
-  if (kind == UK_COND) {
-    u.h = h;
-    if (c0 == 0) {
-      double anorm = 0.0;
-#pragma unroll
-      for (int j = 0; j < RW; ++j) {
-        if constexpr (L::kSplit)
-          anorm = fmax(anorm, part_sum<L::kLanes>(row < N ? cabs(a[j]) : 0.0));
-        else if (j < N)
-          anorm = fmax(anorm, warp_sum(row < N ? cabs(a[j]) : 0.0));
-      }
-      if constexpr (L::kSplit) anorm = warp_max_nonneg(anorm);
-      u.a1 = anorm;
-    }
-    cd r[kCondChunk];
-#pragma unroll
-    for (int q = 0; q < kCondChunk; ++q)
-      r[q] = (row == c0 + q) ? cone<double>() : czero<double>();
-    if (!eliminate<NM, kCondChunk, double>(a, r, N, lane, ws.piv)) {
-      u.ok = false;  // cond1 of an exactly singular matrix
+      for (int j = 0; j < RW; ++j) rs += cabs(a[j]);
+      rs = row_sum<L::kLanes>(rs);
+      u.a1 = warp_max_nonneg(row < N ? cabs(h) : 0.0);
+      u.a2 = warp_max_nonneg(row < N ? rs : 0.0);
+      u.ok = true;
       return;
     }
-    double ainv = 0.0;
+    if (kind == UK_COND) {
+      u.h = h;
+      if (c0 == 0) {
+        double anorm = 0.0;
 #pragma unroll
-    for (int q = 0; q < kCondChunk; ++q) {
-      if (c0 + q < N) ainv = fmax(ainv, warp_sum(owner && row < N ? cabs(r[q]) : 0.0));
+        for (int j = 0; j < RW; ++j) {
+          if constexpr (L::kSplit)
+            anorm = fmax(anorm, part_sum<L::kLanes>(row < N ? cabs(a[j]) : 0.0));
+          else if (j < N)
+            anorm = fmax(anorm, warp_sum(row < N ? cabs(a[j]) : 0.0));
+        }
+        if constexpr (L::kSplit) anorm = warp_max_nonneg(anorm);
+        u.a1 = anorm;
+      }
+      cd r[kCondChunk];
+#pragma unroll
+      for (int q = 0; q < kCondChunk; ++q)
+        r[q] = (row == c0 + q) ? cone<double>() : czero<double>();
+      if (!eliminate<NM, kCondChunk, double>(a, r, N, lane, ws.piv)) {
+        u.ok = false;  // cond1 of an exactly singular matrix
+        return;
+      }
+      double ainv = 0.0;
+#pragma unroll
+      for (int q = 0; q < kCondChunk; ++q) {
+        if (c0 + q < N) ainv = fmax(ainv, warp_sum(owner && row < N ? cabs(r[q]) : 0.0));
+      }
+      u.a2 = ainv;
+      u.ok = true;
+      return;
     }
-    u.a2 = ainv;
-    u.ok = true;
-    return;
-  }
-  if (!MIXED || prec == 0) {
-    cd r[1];
-    r[0] = (kind == UK_TANGENT) ? -(ht * dt) : -h;
-    u.ok = eliminate<NM, 1, double>(a, r, N, lane, ws.piv);
-    if (!u.ok) return;
-    const cd x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
-    u.x = (lane < N) ? x : czero<double>();
-    return;
-  }
-  // mixed predictor and corrector: FP64 evaluation, FP32 elimination
-  if constexpr (MIXED) {
-    cpx<float> as[RW];
+    if (!MIXED || prec == 0) {
+      cd r[1];
+      r[0] = (kind == UK_TANGENT) ? -(ht * dt) : -h;
+      u.ok = eliminate<NM, 1, double>(a, r, N, lane, ws.piv);
+      if (!u.ok) return;
+      const cd x = shfl(r[0], ws.piv[lane < N ? lane : 0]);
+      u.x = (lane < N) ? x : czero<double>();
+      return;
+    }
+    // FP64 evaluation, FP32 elimination
+    if constexpr (MIXED) {
 #pragma unroll
-    for (int j = 0; j < RW; ++j) as[j] = ccast<float>(a[j]);
+      for (int j = 0; j < RW; ++j) as[j] = ccast<float>(a[j]);
+    }
+  } else if constexpr (MIXED && EVAL32) {
+    evaluate_rows<NM, float, F>(C, ws, zin, t, lane, as, h, ht);
+  }
+  if constexpr (MIXED) {
     cpx<float> r[1];
     r[0] = ccast<float>((kind == UK_TANGENT) ? -(ht * dt) : -h);
     u.ok = eliminate<NM, 1, float>(as, r, N, lane, ws.piv);
@@ -252,7 +265,7 @@ __device__ __forceinline__ double vnorm2(cd v, int lane, int N) {
 #define STV(f, v) sts(&LV(f), (v))
 
 // Tracks path k (1-based) and writes its record, z and x.
-template <int NM, int PREC, int F>
+template <int NM, int PREC, bool EVAL32, int F>
 __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& C,
                                           const WarpWS& ws, WarpState& st, const KOpts& O,
                                           int64_t k, int lane, phc_path_out* rec, double* zo,
@@ -270,7 +283,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
   bool att64 = true;
   // pending unit
   int uk = UK_TANGENT, pc_after = PC_FINISH;
-  int u_prec = 0;  // 0: FP64 elimination, 1: FP32 elimination (the evaluation is FP64)
+  int u_prec = 0;  // 0: FP64, 1: FP64 evaluation + FP32 elimination, 2: FP32 evaluation + elimination
   cd tin = z, dtin = z;
   UnitRes U;
   U.x = U.h = czero<double>();
@@ -358,7 +371,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           // predict_rk4 stage 1: tangent at (z, s), src/tracker.f90:283
           stage = 0;
           uk = UK_TANGENT;
-          u_prec = att64 ? 0 : 1;
+          u_prec = att64 ? 0 : (EVAL32 ? 2 : 1);
           zin = zs;
           seg_tdt(st, s, tin, dtin);
           pc_after = PC_SEG_AFTER_UNIT;
@@ -906,7 +919,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
       }
     }
     // ---- run the requested unit ----
-    run_unit<NM, kMixed, F>(C, ws, uk, kMixed ? u_prec : 0, st.cond_c0, zin, tin, dtin, lane,
+    run_unit<NM, kMixed, EVAL32, F>(C, ws, uk, kMixed ? u_prec : 0, st.cond_c0, zin, tin, dtin, lane,
                             U);
     if (kMixed && u_prec == 0 && uk <= UK_NEWTON) ++st.c_retry;  // predictor/corrector unit in FP64
     ++st.units;
@@ -922,10 +935,12 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
 template <int PREC>
 __device__ __forceinline__ WarpWS warp_workspace(const PlanHeader& P, unsigned char* wbase,
                                                 WarpState** st) {
-  const WsLayout L = ws_layout(P.n, P.S, P.pw_total);
+  const WsLayout L = ws_layout(P.n, P.S, P.pw_total, PREC == PHC_PREC_MIXED);
   WarpWS ws;
   ws.pwd = reinterpret_cast<cd*>(wbase + L.pwd);
+  ws.pwf = reinterpret_cast<cf*>(wbase + L.pwf);
   ws.jd = reinterpret_cast<cd*>(wbase + L.jd);
+  ws.jf = reinterpret_cast<cf*>(wbase + L.jf);
   ws.piv = reinterpret_cast<int*>(wbase + L.piv);
   *st = reinterpret_cast<WarpState*>(wbase + L.st);
   return ws;
@@ -942,6 +957,7 @@ __device__ __forceinline__ void init_jacobian_buffer(const PlanHeader& P, const 
     cd v = czero<double>();
     if (row == P.n && col < P.N) v = mkc<double>(P.patch[col][0], P.patch[col][1]);
     sts(&ws.jd[q], v);
+    if (PREC == PHC_PREC_MIXED) sts(&ws.jf[q], ccast<float>(v));
   }
   __syncwarp();
 }
@@ -984,7 +1000,8 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
       qend = q + 1;
       if (q >= kp.count) break;
     }
-    track_one<NM, PREC, F>(P, C, ws, *stp, kp.opts, kp.k0 + q, lane, kp.out + q,
+    track_one<NM, PREC, PREC == PHC_PREC_MIXED && NM <= 8, F>(P, C, ws, *stp, kp.opts, kp.k0 + q,
+                                                             lane, kp.out + q,
                         kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
   }
 }
@@ -1049,7 +1066,7 @@ __global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb)
     phc_path_out* out = reinterpret_cast<phc_path_out*>(kb.base + S.out_off) + kl;
     double* z = reinterpret_cast<double*>(kb.base + S.z_off) + 2 * kl * N;
     double* x = S.x_off >= 0 ? reinterpret_cast<double*>(kb.base + S.x_off) + 2 * kl * n : nullptr;
-    track_one<NM, PREC, F>(P, C, ws, *stp, *opts, kl + 1, lane, out, z, x);
+    track_one<NM, PREC, false, F>(P, C, ws, *stp, *opts, kl + 1, lane, out, z, x);
     if (kb.done != nullptr) {
       // every lane's result stores are made visible system-wide before the
       // path is counted as finished

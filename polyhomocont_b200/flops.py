@@ -17,7 +17,8 @@ corrector and refine units cost F_unit, evaluation-only units F_eval + F_hom,
 a cond1 call F_LU + N F_sol. In mixed precision a predictor or corrector
 unit evaluates H, H_z and H_t in FP64 (F_eval + F_hom) and eliminates in
 FP32 (F_LU + F_sol), unless the whole unit ran in FP64 (counter
-n_fp64_retry).
+n_fp64_retry). (The single-system kernels for n <= 7 evaluate the mixed
+predictor in FP32; the model counts that evaluation as FP64.)
 """
 import numpy as np
 
