@@ -292,7 +292,8 @@ def _fill_result(n, npaths, bufs, rc):
 
 def solve(sys, options=None, gpu=None, buffers=None):
     """solve(sys, res, status, options), src/solve.f90:154-215, on the GPU.
-    sys is a SparseSystem or a PolySystem (sampled first). Returns (res, status); status is err_invalid_input for systems the
+    sys is a SparseSystem or a PolySystem (sampled first). Returns
+    (res, status); status is err_invalid_input for systems the
     reference rejects. Device errors raise PhcError. buffers: optional
     (bufs, rc) from _result_buffers, reused across calls."""
     L = _abi.lib()
