@@ -144,23 +144,51 @@ def test_check_user_system_on_the_restatement(orc):
     assert ru.nduplicates == 0
 
 
+def _by_hand(z):
+    """homogenized_by_hand, test/system.f90:65-80"""
+    w = z[2]
+    f = np.array([z[0] ** 2 + z[1] ** 2 - 5 * w ** 2,
+                  z[0] * z[1] ** 2 - 2 * z[1] * w ** 2 + z[0] * w ** 2])
+    jac = np.array([[2 * z[0], 2 * z[1], -10 * w],
+                    [z[1] ** 2 + w ** 2, 2 * z[0] * z[1] - 2 * w ** 2,
+                     -4 * z[1] * w + 2 * z[0] * w]])
+    return f, jac
+
+
 def test_default_homogenization_matches_by_hand(orc):
-    """test/system.f90:108-125: the default homogenization against the
-    homogenized system written out by hand, at a generic point and at one
-    close to infinity."""
+    """test/system.f90:104-138 on the restatement's default homogenization:
+    against the system homogenized by hand, by finite differences and by
+    homogeneity at a generic point, and against the hand-written system
+    close to infinity (w = 1e-6 - 2e-6 i, where dF^h/dw loses about
+    eps/|w| to cancellation), with the reference's tolerances."""
     u = orc.UserSystem(ClosedForm())
-    for z in ([0.3 - 1.2j, 2.1 + 0.4j, 0.7 + 0.2j], [0.3 - 1.2j, 2.1 + 0.4j, 1e-6 + 2e-6j]):
-        z = np.array(z)
-        f, jac = u.evaluate_homogeneous(z)
-        w = z[2]
-        fr = np.array([z[0] ** 2 + z[1] ** 2 - 5 * w ** 2,
-                       z[0] * z[1] ** 2 - 2 * z[1] * w ** 2 + z[0] * w ** 2])
-        jr = np.array([[2 * z[0], 2 * z[1], -10 * w],
-                       [z[1] ** 2 + w ** 2, 2 * z[0] * z[1] - 2 * w ** 2,
-                        -4 * z[1] * w + 2 * z[0] * w]])
-        scale = max(1.0, np.max(np.abs(z))) ** 3
-        assert np.max(np.abs(f - fr)) <= 1e-12 * scale
-        assert np.max(np.abs(jac - jr)) <= 1e-10 * scale
+    z = np.array([0.3 - 1.2j, 2.1 + 0.4j, 0.7 + 0.2j])
+    f, jac = u.evaluate_homogeneous(z)
+    fr, jr = _by_hand(z)
+    assert np.max(np.abs(f - fr)) <= 1e-13
+    assert np.max(np.abs(jac - jr)) <= 1e-13
+    # homogeneous_jacobian_fd_error, test/testing.f90:158-188
+    err = 0.0
+    for j in range(3):
+        h = 1e-5 * max(1.0, abs(z[j]))
+        zp, zm = z.copy(), z.copy()
+        zp[j] += h
+        zm[j] -= h
+        err = max(err, np.max(np.abs((u.evaluate_homogeneous(zp)[0] -
+                                      u.evaluate_homogeneous(zm)[0]) / (2 * h) - jac[:, j])))
+    assert err / max(1.0, np.max(np.abs(jac))) <= 1e-8
+    # homogeneity_error, test/testing.f90:190-215, lambda = 0.6 - 1.3 i
+    lam, d = 0.6 - 1.3j, np.array([2, 3])
+    fl, _ = u.evaluate_homogeneous(lam * z)
+    fa, _ = ClosedForm().evaluate(z[:2] / z[2])
+    herr = max(np.max(np.abs(fl - lam ** d * f)) / max(1.0, np.max(np.abs(fl))),
+               np.max(np.abs(f - z[2] ** d * fa)) / max(1.0, np.max(np.abs(f))))
+    assert herr <= 1e-13
+    z[2] = 1e-6 - 2e-6j
+    f, jac = u.evaluate_homogeneous(z)
+    fr, jr = _by_hand(z)
+    assert np.max(np.abs(f - fr)) / np.max(np.abs(fr)) <= 1e-9
+    assert np.max(np.abs(jac - jr)) / np.max(np.abs(jr)) <= 1e-8
 
 
 def test_circle_cubic_example_on_the_restatement(orc):
