@@ -19,7 +19,8 @@ namespace {
 struct Contribution {
   double cre, cim;
   int dest;
-  std::vector<int> fac;  // power-table offsets e*N + j
+  int nf;             // factors in use
+  int fac[kMaxN];     // power-table offsets e*N + j (at most N before reduction)
 };
 
 struct PackedRec {
@@ -35,16 +36,25 @@ uint64_t pack_meta(int dest, int nf, unsigned flags, const int* fac) {
   return m;
 }
 
+// Contributions of all entries in one array, entry by entry (entry e owns
+// cs[off[e] .. off[e+1]), in term order).
+struct Entries {
+  std::vector<int> off;
+  std::vector<Contribution> cs;
+  int count() const { return (int)off.size() - 1; }
+  int size(int e) const { return off[e + 1] - off[e]; }
+};
+
 // Appends the records of one entry (its contributions in term order);
 // every contribution has at most kMaxFac factors at this point.
-void emit_entry(const std::vector<Contribution>& cs, std::vector<PackedRec>& out) {
-  for (size_t c = 0; c < cs.size(); ++c) {
-    const Contribution& C = cs[c];
-    const unsigned flags = (c + 1 == cs.size()) ? kRecLast : 0u;
+void emit_entry(const Entries& E, int e, std::vector<PackedRec>& out) {
+  for (int c = E.off[e]; c < E.off[e + 1]; ++c) {
+    const Contribution& C = E.cs[c];
+    const unsigned flags = (c + 1 == E.off[e + 1]) ? kRecLast : 0u;
     PackedRec r;
     r.cre = C.cre;
     r.cim = C.cim;
-    r.meta = pack_meta(C.dest, (int)C.fac.size(), flags, C.fac.data());
+    r.meta = pack_meta(C.dest, C.nf, flags, C.fac);
     out.push_back(r);
   }
 }
@@ -68,45 +78,44 @@ struct PreTable {
     index[t] = e;
     return e;
   }
-  void reduce(std::vector<int>& fac) {
-    while (fac.size() > (size_t)kMaxFac) {
-      std::array<int, 3> t = {fac[0], fac[1], fac[2]};
-      const int e = intern(t);
-      fac.erase(fac.begin(), fac.begin() + 3);
-      fac.insert(fac.begin(), e);
+  // replaces the first three factors by their extended entry until at
+  // most kMaxFac remain
+  void reduce(int* fac, int& nf) {
+    while (nf > kMaxFac) {
+      const std::array<int, 3> t = {fac[0], fac[1], fac[2]};
+      fac[0] = intern(t);
+      std::memmove(fac + 1, fac + 3, sizeof(int) * (size_t)(nf - 3));
+      nf -= 2;
     }
   }
 };
 
 // Longest-processing-time assignment of entries to the 32 lanes; each lane
 // gets its entries in increasing entry order.
-void schedule(const std::vector<std::vector<Contribution>>& entries,
-              std::vector<std::vector<PackedRec>>& lanes) {
-  const int ne = (int)entries.size();
+void schedule(const Entries& E, std::vector<std::vector<PackedRec>>& lanes) {
+  const int ne = E.count();
   std::vector<long> cost(ne, 0);
   for (int e = 0; e < ne; ++e)
-    for (const auto& c : entries[e]) cost[e] += 3 + (long)c.fac.size();
+    for (int c = E.off[e]; c < E.off[e + 1]; ++c) cost[e] += 3 + (long)E.cs[c].nf;
   std::vector<int> order(ne);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return cost[a] > cost[b]; });
-  std::vector<long> load(kWarp, 0);
-  std::vector<std::vector<int>> lane_entries(kWarp);
+  long load[kWarp] = {}, recs[kWarp] = {};
+  std::vector<int> lane_of(ne, -1);  // lane of each entry (-1: empty entry)
   for (int e : order) {
-    if (entries[e].empty()) continue;
+    if (E.size(e) == 0) continue;
     int best = 0;
     for (int l = 1; l < kWarp; ++l)
       if (load[l] < load[best]) best = l;
     load[best] += cost[e];
-    lane_entries[best].push_back(e);
+    lane_of[e] = best;
+    recs[best] += E.size(e);
   }
   // The kernel runs every lane for the longest lane's record count rounded
   // up to a multiple of 4. If the LPT assignment misses the next lower
   // multiple of 4, try to pack the entries into lanes of that many records
   // (best fit, largest entries first); keep it when everything fits.
-  std::vector<long> recs(kWarp, 0);
-  for (int l = 0; l < kWarp; ++l)
-    for (int e : lane_entries[l]) recs[l] += (long)entries[e].size();
   long total = 0, lpt_max = 0;
   for (int l = 0; l < kWarp; ++l) {
     total += recs[l];
@@ -115,14 +124,13 @@ void schedule(const std::vector<std::vector<Contribution>>& entries,
   const long target = ((lpt_max + 3) & ~3L) - 4;
   if (target > 0 && target * kWarp >= total) {
     std::vector<int> by_size(order);
-    std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int b) {
-      return entries[a].size() > entries[b].size();
-    });
-    std::vector<long> fill(kWarp, 0);
-    std::vector<std::vector<int>> packed(kWarp);
+    std::stable_sort(by_size.begin(), by_size.end(),
+                     [&](int a, int b) { return E.size(a) > E.size(b); });
+    long fill[kWarp] = {};
+    std::vector<int> packed(ne, -1);
     bool ok = true;
     for (int e : by_size) {
-      const long sz = (long)entries[e].size();
+      const long sz = (long)E.size(e);
       if (sz == 0) continue;
       int best = -1;
       for (int l = 0; l < kWarp; ++l)
@@ -132,15 +140,17 @@ void schedule(const std::vector<std::vector<Contribution>>& entries,
         break;
       }
       fill[best] += sz;
-      packed[best].push_back(e);
+      packed[e] = best;
     }
-    if (ok) lane_entries.swap(packed);
+    if (ok) {
+      lane_of.swap(packed);
+      for (int l = 0; l < kWarp; ++l) recs[l] = fill[l];
+    }
   }
   lanes.assign(kWarp, {});
-  for (int l = 0; l < kWarp; ++l) {
-    std::sort(lane_entries[l].begin(), lane_entries[l].end());
-    for (int e : lane_entries[l]) emit_entry(entries[e], lanes[l]);
-  }
+  for (int l = 0; l < kWarp; ++l) lanes[l].reserve((size_t)recs[l]);
+  for (int e = 0; e < ne; ++e)
+    if (lane_of[e] >= 0) emit_entry(E, e, lanes[lane_of[e]]);
 }
 
 // Writes one schedule's lane-interleaved arrays at the given offsets.
@@ -339,32 +349,45 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   // Jacobian contributions per entry, in term order (eval_terms,
   // src/sparse.f90:259-278). F^h itself is not tabulated: the kernel
   // obtains it from the Jacobian row by Euler's relation.
-  std::vector<std::vector<Contribution>> fent(0), jent((size_t)n * S);
+  // (two passes: count the contributions of each entry, then fill them in
+  // term order into one array)
+  Entries fent, jent;
+  fent.off.assign(1, 0);
+  const int ne = n * S;
+  jent.off.assign((size_t)ne + 1, 0);
+  for (int i = 0; i < n; ++i)
+    for (int k = sys->first[i]; k < sys->first[i + 1]; ++k) {
+      const int* e = sys->hexps + (size_t)k * N;
+      for (int j = 0; j < N; ++j)
+        if (e[j] > 0) ++jent.off[(size_t)i * S + j + 1];
+    }
+  for (int q = 0; q < ne; ++q) jent.off[q + 1] += jent.off[q];
+  jent.cs.resize((size_t)jent.off[ne]);
+  std::vector<int> fill(jent.off.begin(), jent.off.end() - 1);
   for (int i = 0; i < n; ++i) {
     for (int k = sys->first[i]; k < sys->first[i + 1]; ++k) {
       const int* e = sys->hexps + (size_t)k * N;
       const double cre = sys->coefs[2 * k], cim = sys->coefs[2 * k + 1];
       for (int j = 0; j < N; ++j) {
         if (e[j] <= 0) continue;
-        Contribution d;
+        Contribution& d = jent.cs[fill[(size_t)i * S + j]++];
         d.cre = (double)e[j] * cre;
         d.cim = (double)e[j] * cim;
         d.dest = i * S + j;
-        if (e[j] > 1) d.fac.push_back((e[j] - 1) * N + j);
+        d.nf = 0;
+        if (e[j] > 1) d.fac[d.nf++] = (e[j] - 1) * N + j;
         for (int l = 0; l < N; ++l)
-          if (l != j && e[l] > 0) d.fac.push_back(e[l] * N + l);
-        jent[(size_t)i * S + j].push_back(d);
+          if (l != j && e[l] > 0) d.fac[d.nf++] = e[l] * N + l;
       }
     }
   }
   PreTable pre;
   pre.base = pw_size;
   int max_fac = 0;
-  for (auto& ent : jent)
-    for (auto& c : ent) {
-      pre.reduce(c.fac);
-      max_fac = std::max(max_fac, (int)c.fac.size());
-    }
+  for (auto& c : jent.cs) {
+    pre.reduce(c.fac, c.nf);
+    max_fac = std::max(max_fac, c.nf);
+  }
   H.max_fac = max_fac;
   const int n_pre = (int)pre.entries.size();
   int n_levels = 0;
