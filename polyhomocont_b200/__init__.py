@@ -482,63 +482,22 @@ class Plan:
 
 def result_from_arrays(n, paths, x, options=None):
     """Host bookkeeping of solve() (add_solution, add_singular, find,
-    collect_real) applied to per-path records, in path order. Mirrors
-    src/solve.f90:193-213, :330-426; used when paths were produced by a
-    device-resident plan."""
+    collect_real; src/solve.f90:193-213, :330-426) applied to per-path
+    records in path order, through the library (phc_finish_solve): for
+    paths produced by device-resident plans or gathered from several
+    GPUs. z of the result is left zero."""
+    L = _abi.lib()
     o = options if options is not None else default_options()
-    paths = np.array(paths, dtype=PATH_DTYPE, copy=True)
-    x = np.ascontiguousarray(x, dtype=np.complex128)
-    res = SolveResult()
-    res.n = n
-    res.npaths = len(paths)
-    res.paths = paths
-
-    def norm_inf(v):
-        return float(np.max(np.abs(v))) if len(v) else 0.0
-
-    def find(v, pts, tol):
-        scale = max(1.0, norm_inf(v))
-        for j, p in enumerate(pts):
-            if norm_inf(v - p) <= tol * scale:
-                return j + 1
-        return 0
-
-    sols, ssols, mult = [], [], []
-    for k in range(len(paths)):
-        p = paths[k]
-        p["solution_index"] = 0
-        p["singular_index"] = 0
-        if p["status"] != PATH_SUCCESS:
-            res.nfailed += 1
-        elif p["at_infinity"]:
-            res.ninfinite += 1
-        elif p["singular"]:
-            j = find(x[k], ssols, o.singular_dedup_tol)
-            if j > 0:
-                mult[j - 1] += 1
-            else:
-                ssols.append(x[k].copy())
-                mult.append(1)
-                j = len(ssols)
-            p["singular_index"] = j
-        else:
-            j = find(x[k], sols, o.dedup_tol)
-            if j > 0:
-                res.nduplicates += 1
-            else:
-                sols.append(x[k].copy())
-                j = len(sols)
-            p["solution_index"] = j
-    res.nsolutions = len(sols)
-    res.solutions = np.array(sols, dtype=np.complex128).reshape(len(sols), n)
-    res.nsingular = len(ssols)
-    res.singular_solutions = np.array(ssols, dtype=np.complex128).reshape(len(ssols), n)
-    res.multiplicities = np.array(mult, dtype=np.int32)
-    reals = [s.real for s in sols
-             if np.max(np.abs(s.imag)) <= o.real_tol * max(1.0, norm_inf(s))]
-    res.nreal = len(reals)
-    res.real_solutions = np.array(reals).reshape(len(reals), n)
-    return res
+    npaths = len(paths)
+    bufs, rc = _result_buffers(n, npaths)
+    bufs["paths"][:npaths] = paths
+    bufs["x"][:npaths, :n] = x
+    st = L.phc_finish_solve(int(n), int(npaths), ctypes.byref(o),
+                            bufs["paths"].ctypes.data_as(ctypes.c_void_p),
+                            _abi.dptr(bufs["x"].view(np.float64)), ctypes.byref(rc))
+    if st != PHC_OK:
+        raise PhcError(st, "phc_finish_solve")
+    return _fill_result(n, npaths, bufs, rc)
 
 
 class Server:

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <limits>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -378,6 +379,20 @@ static double norm_inf_c(const double* v, int n) {
   return r;
 }
 
+// The square root of the largest squared modulus: within a few ulps of
+// norm_inf, without a hypot. NaN when a square could over- or underflow
+// or a value is not finite; the caller then takes the exact norm.
+static double norm_inf_estimate(const double* v, int n) {
+  double m2 = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double s = v[2 * i] * v[2 * i] + v[2 * i + 1] * v[2 * i + 1];
+    if (!(s <= kSqHi)) return std::numeric_limits<double>::quiet_NaN();
+    m2 = std::max(m2, s);
+  }
+  if (m2 < kSqLo) return std::numeric_limits<double>::quiet_NaN();
+  return std::sqrt(m2);
+}
+
 // The reference's find (src/solve.f90:379-400) scans all stored points and
 // returns the first (lowest index) within tol * max(1, ||x||). PointSet
 // returns the same index without the O(P) scan: any match lies within the
@@ -401,14 +416,23 @@ class PointSet {
   int size() const { return (int)rows_.size(); }
   const double* point(int j) const { return x_ + (size_t)rows_[j] * 2 * n_; }
 
+  // rho = tol * max(1, ||x||) comes from the norm estimate; the decisions
+  // it makes keep a relative margin of 1e-12, far above the estimate's
+  // error, and the few comparisons inside the margin use the exact norm.
   int find(const double* x) const {
-    const double scale = std::max(1.0, norm_inf_c(x, n_));
-    const double rho = tol_ * scale;
+    const double est = norm_inf_estimate(x, n_);
+    const bool approx = std::isfinite(est);
+    const double rho = tol_ * std::max(1.0, approx ? est : norm_inf_c(x, n_));
+    double rho_exact = approx ? -1.0 : rho;  // computed on first need
+    auto exact_rho = [&]() {
+      if (rho_exact < 0.0) rho_exact = tol_ * std::max(1.0, norm_inf_c(x, n_));
+      return rho_exact;
+    };
     const double x0 = x[0];
     int best = -1;
     auto test = [&](int j) {
       if (best >= 0 && j >= best) return;
-      if (within(x, j, rho)) best = j;
+      if (within(x, j, rho, exact_rho)) best = j;
     };
     const double margin = 1e-12 * (std::fabs(x0) + rho) + 1e-300;
     const double lo = x0 - rho - margin, hi = x0 + rho + margin;
@@ -475,8 +499,10 @@ class PointSet {
       heads_[t] = h2[s];
     }
   }
-  // max_i |x_i - p_i| <= rho, decided on squares away from the threshold
-  bool within(const double* x, int j, double rho) const {
+  // max_i |x_i - p_i| <= rho, decided on squares away from the threshold;
+  // at the threshold, hypot distances against the exact rho
+  template <class ExactRho>
+  bool within(const double* x, int j, double rho, ExactRho&& exact_rho) const {
     const double* p = point(j);
     const double r2 = rho * rho;
     bool exact = !(r2 >= kSqLo && r2 <= kSqHi);
@@ -494,7 +520,7 @@ class PointSet {
     double d = 0.0;
     for (int i = 0; i < n_; ++i)
       d = std::max(d, std::hypot(x[2 * i] - p[2 * i], x[2 * i + 1] - p[2 * i + 1]));
-    return d <= rho;
+    return d <= exact_rho();
   }
   int n_;
   double tol_, width_;
@@ -559,7 +585,17 @@ void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out
     const double* sj = sols.point(j);
     double imax = 0.0;
     for (int i = 0; i < n; ++i) imax = std::max(imax, std::fabs(sj[2 * i + 1]));
-    if (imax <= o.real_tol * std::max(1.0, norm_inf_c(sj, n))) {
+    // imax <= real_tol * max(1, ||s||), the norm estimated away from the threshold
+    const double est = norm_inf_estimate(sj, n);
+    bool real;
+    const double thr = o.real_tol * std::max(1.0, est);
+    if (std::isfinite(est) && imax <= thr * (1.0 - kSqMargin))
+      real = true;
+    else if (std::isfinite(est) && imax >= thr * (1.0 + kSqMargin))
+      real = false;
+    else
+      real = imax <= o.real_tol * std::max(1.0, norm_inf_c(sj, n));
+    if (real) {
       if (res->real_solutions)
         for (int i = 0; i < n; ++i) res->real_solutions[(size_t)nreal * n + i] = sj[2 * i];
       ++nreal;

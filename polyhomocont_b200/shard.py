@@ -7,11 +7,7 @@ are gathered to rank 0 in global path order, and rank 0 runs the
 order-dependent host bookkeeping (phc_finish_solve), which makes the result
 identical to a single-GPU solve.
 """
-import ctypes
-
 import numpy as np
-
-from . import _abi
 
 
 def path_range(npaths, rank, world):
@@ -24,20 +20,8 @@ def path_range(npaths, rank, world):
 
 def finish_solve(n, paths, x, options=None):
     """Host bookkeeping on gathered records (phc_finish_solve)."""
-    from . import SolveResult, _fill_result, _result_buffers, default_options
-    L = _abi.lib()
-    o = options if options is not None else default_options()
-    npaths = len(paths)
-    bufs, rc = _result_buffers(n, npaths)
-    bufs["paths"][:npaths] = paths
-    bufs["x"][:npaths, :n] = x
-    st = L.phc_finish_solve(int(n), int(npaths), ctypes.byref(o),
-                            bufs["paths"].ctypes.data_as(ctypes.c_void_p),
-                            _abi.dptr(bufs["x"].view(np.float64)), ctypes.byref(rc))
-    if st != 0:
-        raise RuntimeError(f"phc_finish_solve: {st}")
-    res = _fill_result(n, npaths, bufs, rc)
-    return res
+    from . import result_from_arrays
+    return result_from_arrays(n, paths, x, options)
 
 
 class ShardFailure(RuntimeError):

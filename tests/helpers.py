@@ -103,3 +103,58 @@ class TermEvaluator:
                 d[j] = np.maximum(d[j] - 1, 0)
                 jac[i, j] = np.sum(c * e[j] * np.prod(x[:, None] ** d, axis=0))
         return f, jac
+
+
+def reference_bookkeeping(n, paths, x, o):
+    """add_solution, add_singular, find and collect_real of the reference
+    (src/solve.f90:330-426), restated directly in path order: the first
+    stored point within tol * max(1, ||x||_inf) of x by max-norm distance
+    (moduli as hypot). Returns a dict of the counts, per-path indices,
+    solution arrays and multiplicities. Moduli come from np.hypot on the
+    real and imaginary parts, which matches the C library's hypot (the
+    modulus of Fortran's abs); numpy's complex abs is off by one ulp for
+    some inputs, which flips decisions that sit exactly at a threshold."""
+    def norm_inf(v):
+        return float(np.max(np.hypot(v.real, v.imag))) if len(v) else 0.0
+
+    def find(v, pts, tol):
+        scale = max(1.0, norm_inf(v))
+        for j, p in enumerate(pts):
+            if norm_inf(v - p) <= tol * scale:
+                return j + 1
+        return 0
+
+    sols, ssols, mult = [], [], []
+    sol_idx = np.zeros(len(paths), dtype=np.int32)
+    sing_idx = np.zeros(len(paths), dtype=np.int32)
+    nfailed = ninfinite = nduplicates = 0
+    for k in range(len(paths)):
+        p = paths[k]
+        if p["status"] != 0:
+            nfailed += 1
+        elif p["at_infinity"]:
+            ninfinite += 1
+        elif p["singular"]:
+            j = find(x[k], ssols, o.singular_dedup_tol)
+            if j > 0:
+                mult[j - 1] += 1
+            else:
+                ssols.append(x[k].copy())
+                mult.append(1)
+                j = len(ssols)
+            sing_idx[k] = j
+        else:
+            j = find(x[k], sols, o.dedup_tol)
+            if j > 0:
+                nduplicates += 1
+            else:
+                sols.append(x[k].copy())
+                j = len(sols)
+            sol_idx[k] = j
+    reals = [s.real for s in sols if np.max(np.abs(s.imag)) <= o.real_tol * max(1.0, norm_inf(s))]
+    return dict(nfailed=nfailed, ninfinite=ninfinite, nduplicates=nduplicates,
+                solution_index=sol_idx, singular_index=sing_idx,
+                solutions=np.array(sols, dtype=np.complex128).reshape(len(sols), n),
+                singular_solutions=np.array(ssols, dtype=np.complex128).reshape(len(ssols), n),
+                multiplicities=np.array(mult, dtype=np.int32),
+                real_solutions=np.array(reals).reshape(len(reals), n))
