@@ -37,7 +37,10 @@
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <condition_variable>
 #include <map>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "phc_host.h"
@@ -108,35 +111,86 @@ void power_table(const cd* x, int n, int d, std::vector<cd>& pw) {
     for (int e = 1; e <= d; ++e) pw[j * (d + 1) + e] = pw[j * (d + 1) + e - 1] * x[j];
 }
 
+// A reusable barrier for a fixed set of threads.
+class Barrier {
+ public:
+  explicit Barrier(int n) : n_(n) {}
+  void wait() {
+    std::unique_lock<std::mutex> lk(mu_);
+    const long gen = gen_;
+    if (++count_ == n_) {
+      count_ = 0;
+      ++gen_;
+      cv_.notify_all();
+      return;
+    }
+    cv_.wait(lk, [&] { return gen_ != gen; });
+  }
+
+ private:
+  std::mutex mu_;
+  std::condition_variable cv_;
+  int n_, count_ = 0;
+  long gen_ = 0;
+};
+
 // Least squares min ||A X - B|| for A rows x cols (rows >= cols) and B
 // rows x nrhs, both column-major, by Householder QR applied to B as the
 // reflections are formed; X overwrites the first cols rows of B. Returns
 // false when R has a negligible diagonal entry (rank-deficient design).
+// For large designs each reflection is applied to the remaining columns
+// by up to 16 threads, each column by one thread in the serial order of
+// operations, so the result does not depend on the thread count.
 bool least_squares(std::vector<cd>& A, int rows, int cols, std::vector<cd>& B, int nrhs) {
   std::vector<cd> diag(cols);
-  double dmax = 0.0;
-  for (int k = 0; k < cols; ++k) {
-    cd* a = &A[(size_t)k * rows];
-    double ss = 0.0;
-    for (int i = k; i < rows; ++i) ss += std::norm(a[i]);
-    const double s = std::sqrt(ss);
-    if (s == 0.0) return false;
-    const double ak = std::abs(a[k]);
-    const cd alpha = ak == 0.0 ? cd(-s) : -(a[k] / ak) * s;
-    a[k] -= alpha;  // v = x - alpha e_k, kept in column k below the diagonal
-    double vv = 0.0;
-    for (int i = k; i < rows; ++i) vv += std::norm(a[i]);
-    auto reflect = [&](cd* y) {
-      cd dot = 0.0;
-      for (int i = k; i < rows; ++i) dot += std::conj(a[i]) * y[i];
-      const cd f = 2.0 * dot / vv;
-      for (int i = k; i < rows; ++i) y[i] -= f * a[i];
-    };
-    for (int c = k + 1; c < cols; ++c) reflect(&A[(size_t)c * rows]);
-    for (int r = 0; r < nrhs; ++r) reflect(&B[(size_t)r * rows]);
-    diag[k] = alpha;
-    dmax = std::max(dmax, s);
+  double dmax = 0.0, vv = 0.0;
+  bool failed = false;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int T = cols >= 192 ? (int)std::min(hw, 16u) : 1;
+  Barrier bar(T);
+  auto work = [&](int t) {
+    for (int k = 0; k < cols; ++k) {
+      cd* a = &A[(size_t)k * rows];
+      if (t == 0) {  // the reflection of column k: v = x - alpha e_k in place
+        double ss = 0.0;
+        for (int i = k; i < rows; ++i) ss += std::norm(a[i]);
+        const double s = std::sqrt(ss);
+        if (s == 0.0) {
+          failed = true;
+        } else {
+          const double ak = std::abs(a[k]);
+          const cd alpha = ak == 0.0 ? cd(-s) : -(a[k] / ak) * s;
+          a[k] -= alpha;
+          vv = 0.0;
+          for (int i = k; i < rows; ++i) vv += std::norm(a[i]);
+          diag[k] = alpha;
+          dmax = std::max(dmax, s);
+        }
+      }
+      if (T > 1) bar.wait();
+      if (failed) return;
+      // columns k+1 .. cols-1, then the right-hand sides, in T contiguous ranges
+      const int rest = cols - k - 1, m = rest + nrhs;
+      const int lo = (int)((long)m * t / T), hi = (int)((long)m * (t + 1) / T);
+      for (int q = lo; q < hi; ++q) {
+        cd* y = q < rest ? &A[(size_t)(k + 1 + q) * rows] : &B[(size_t)(q - rest) * rows];
+        cd dot = 0.0;
+        for (int i = k; i < rows; ++i) dot += std::conj(a[i]) * y[i];
+        const cd f = 2.0 * dot / vv;
+        for (int i = k; i < rows; ++i) y[i] -= f * a[i];
+      }
+      if (T > 1) bar.wait();
+    }
+  };
+  if (T == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
   }
+  if (failed) return false;
   for (int k = 0; k < cols; ++k)
     if (std::abs(diag[k]) <= 1e-10 * dmax) return false;
   for (int r = 0; r < nrhs; ++r) {

@@ -78,6 +78,28 @@ Sys random_system(int nmax, int dmax, int tmax) {
   return s;
 }
 
+// n equations of exact degree d with T terms each
+Sys fixed_system(int n, int d, int T) {
+  Sys s;
+  s.n = n;
+  for (int i = 0; i < n; ++i) {
+    std::vector<double> c;
+    std::vector<int32_t> e;
+    for (int k = 0; k < T; ++k) {
+      int left = (k == 0) ? d : uni(0, d);
+      std::vector<int32_t> a(n, 0);
+      while (left-- > 0) a[uni(0, n - 1)] += 1;
+      e.insert(e.end(), a.begin(), a.end());
+      c.push_back(normal());
+      c.push_back(normal());
+    }
+    s.deg.push_back(d);
+    s.coefs.push_back(c);
+    s.exps.push_back(e);
+  }
+  return s;
+}
+
 phc_sparse* build(const Sys& s) {
   phc_sparse* b = phc_sparse_create();
   CHECK(b != nullptr);
@@ -290,6 +312,8 @@ int main(int argc, char** argv) {
     fuzz_wire(a);
     fuzz_bookkeeping();
     if (it % 4 == 0) fuzz_sampler(random_system(5, 3, 8));
+    // 210 monomials of degree <= 4 in 6 unknowns: the threaded least squares
+    if (it % 150 == 0) fuzz_sampler(fixed_system(6, 4, 12));
   }
   std::printf("host_fuzz: %d iterations ok: %ld tables compiled and verified (%ld systems with "
               "too many paths), %ld request round trips, %ld bookkeeping runs, %ld sampled "

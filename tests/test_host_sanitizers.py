@@ -8,7 +8,8 @@ together with every host source of the library (the CUDA objects are linked
 uninstrumented and never called) and run on random systems. It covers the
 table compiler and its verifier, corrupted tables, the request codec with
 damaged requests, the bookkeeping at the dedup tolerance boundaries, and the
-user-system sampler. tests/sanitize/oracle_fuzz.cpp runs the CPU
+user-system sampler; once more under ThreadSanitizer for the sampler's
+threaded least squares. tests/sanitize/oracle_fuzz.cpp runs the CPU
 restatement the same way, and once more under ThreadSanitizer, since its
 solve uses worker threads. Any memory error, undefined behaviour, data race
 or broken invariant fails the run."""
@@ -36,8 +37,7 @@ def _sanitizer_cxx():
     return None
 
 
-@pytest.fixture(scope="module")
-def fuzz_binary(tmp_path_factory):
+def _build_fuzz(tmp_path_factory, sanitize):
     from polyhomocont_b200 import build as B
     B.build()
     cxx = _sanitizer_cxx()
@@ -45,17 +45,24 @@ def fuzz_binary(tmp_path_factory):
         pytest.fail("no C++ compiler with the AddressSanitizer runtime found")
     out = str(tmp_path_factory.mktemp("san") / "host_fuzz")
     csrc = os.path.join(ROOT, "polyhomocont_b200", "csrc")
-    cmd = ([cxx, "-std=c++17", "-O1", "-g", "-fno-omit-frame-pointer",
-            "-fsanitize=address,undefined", "-fno-sanitize-recover=all", "-ffp-contract=off",
+    cmd = ([cxx, "-std=c++17", "-O1", "-g", "-fno-omit-frame-pointer", "-pthread",
+            f"-fsanitize={sanitize}", "-ffp-contract=off",
             "-I", os.path.join(ROOT, "include"), "-I", csrc, "-I", os.path.join(CUDA, "include"),
             os.path.join(ROOT, "tests", "sanitize", "host_fuzz.cpp")]
            + sorted(glob.glob(os.path.join(csrc, "*.cpp")))
            + sorted(glob.glob(os.path.join(B.BUILD, "*.cu.o")))
            + ["-L", os.path.join(CUDA, "lib64"), "-lcudart", "-lpthread", "-ldl", "-lrt",
               "-o", out])
+    if sanitize != "thread":
+        cmd.insert(6, "-fno-sanitize-recover=all")
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stderr[-4000:]
     return out
+
+
+@pytest.fixture(scope="module")
+def fuzz_binary(tmp_path_factory):
+    return _build_fuzz(tmp_path_factory, "address,undefined")
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
@@ -69,6 +76,20 @@ def test_host_code_under_sanitizers(fuzz_binary, seed):
     assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-6000:])
     assert "iterations ok" in r.stdout
     assert "runtime error" not in r.stderr  # UBSan reports
+
+
+def test_host_code_under_thread_sanitizer(tmp_path_factory):
+    """The same driver under ThreadSanitizer: the sampler's least squares
+    runs its column updates on several threads for designs of 192
+    monomials or more (one such design every 150 iterations)."""
+    exe = _build_fuzz(tmp_path_factory, "thread")
+    env = dict(os.environ)
+    env["LD_LIBRARY_PATH"] = os.path.join(CUDA, "lib64") + ":" + env.get("LD_LIBRARY_PATH", "")
+    env["TSAN_OPTIONS"] = "halt_on_error=1"
+    r = subprocess.run([exe, "300", "4"], capture_output=True, text=True, timeout=900, env=env)
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-6000:])
+    assert "iterations ok" in r.stdout
+    assert "WARNING: ThreadSanitizer" not in r.stderr
 
 
 def _build_oracle_driver(tmp_path_factory, cxx, sanitize, name):
