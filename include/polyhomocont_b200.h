@@ -108,8 +108,10 @@ typedef struct {
 /* GPU-only knobs, kept out of phc_solve_options so that it stays a POD
  * mirror of solve_options. A NULL pointer means all defaults. */
 #define PHC_PREC_FP64 0  /* all-FP64 tracker */
-#define PHC_PREC_MIXED 1 /* complex FP32 predictor + Jacobian/LU; FP64 residual,
-                            update, norms, end game decisions, refine, cond1 */
+#define PHC_PREC_MIXED 1 /* complex FP32 eliminations for the predictor and the
+                            corrector (and an FP32 evaluation of the predictor
+                            for n <= 7); FP64 evaluation, residual, update,
+                            norms, end game decisions, refine, cond1 */
 #define PHC_SCHED_GRID 0       /* one warp per path, one launch, no refill */
 #define PHC_SCHED_PERSISTENT 1 /* persistent warps, atomic path queue refill */
 typedef struct {
@@ -218,6 +220,14 @@ int32_t phc_sparse_total_terms(const phc_sparse* s);
 void phc_sparse_degrees(const phc_sparse* s, int32_t* d);  /* :186-195 */
 /* view of the packed table; valid until the builder changes */
 int32_t phc_sparse_table(const phc_sparse* s, phc_system* out);
+/* sys%evaluate(x, f, jac), src/sparse.f90:197-207, on the host: x[2n] and
+ * f[2n] interleaved complex, jac[2 n n] with dF_i/dx_j at complex index
+ * i + j*n (column-major, Fortran's layout) */
+int32_t phc_sparse_evaluate(const phc_sparse* s, const double* x, double* f, double* jac);
+/* sys%evaluate_homogeneous(z, f, jac), src/sparse.f90:209-221: z[2(n+1)]
+ * with w = z_(n+1) last, f[2n], jac[2 n (n+1)]; exact also at w = 0 */
+int32_t phc_sparse_evaluate_homogeneous(const phc_sparse* s, const double* z, double* f,
+                                        double* jac);
 
 /* ---- user-evaluator systems (class(poly_system), src/system.f90:27-67) -- */
 /* sys%evaluate(x, f, jac): x[2n], f[2n] interleaved complex; jac[2 n n] is

@@ -117,6 +117,34 @@ class SparseSystem:
         self._L.phc_sparse_degrees(self.h, _abi.iptr(d))
         return d[:self.nequations()]
 
+    def evaluate(self, x):
+        """sys%evaluate(x, f, jac), src/sparse.f90:197-207: (F(x), dF/dx) with
+        jac[i, j] = dF_i/dx_j (host arithmetic)."""
+        n = self.nvars()
+        xv = np.ascontiguousarray(np.asarray(x, dtype=np.complex128).reshape(n))
+        f = np.zeros(n, dtype=np.complex128)
+        jac = np.zeros((n, n), dtype=np.complex128, order="F")
+        st = self._L.phc_sparse_evaluate(self.h, _abi.dptr(xv.view(np.float64)),
+                                         _abi.dptr(f.view(np.float64)),
+                                         _abi.dptr(jac.reshape(-1, order="F").view(np.float64)))
+        if st != PHC_OK:
+            raise PhcError(st, "phc_sparse_evaluate")
+        return f, jac
+
+    def evaluate_homogeneous(self, z):
+        """sys%evaluate_homogeneous(z, f, jac), src/sparse.f90:209-221:
+        (F^h(z), dF^h/dz) at z = (z_1, ..., z_n, w), exact also at w = 0."""
+        n = self.nvars()
+        zv = np.ascontiguousarray(np.asarray(z, dtype=np.complex128).reshape(n + 1))
+        f = np.zeros(n, dtype=np.complex128)
+        jac = np.zeros((n, n + 1), dtype=np.complex128, order="F")
+        st = self._L.phc_sparse_evaluate_homogeneous(
+            self.h, _abi.dptr(zv.view(np.float64)), _abi.dptr(f.view(np.float64)),
+            _abi.dptr(jac.reshape(-1, order="F").view(np.float64)))
+        if st != PHC_OK:
+            raise PhcError(st, "phc_sparse_evaluate_homogeneous")
+        return f, jac
+
     def table(self):
         """phc_system view of the packed table and its status (err_invalid_input
         if the system does not have n equations)."""

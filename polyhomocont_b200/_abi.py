@@ -129,6 +129,8 @@ SIGNATURES = [
     ("phc_sparse_total_terms", c_i32, [c_vp]),
     ("phc_sparse_degrees", None, [c_vp, P(c_i32)]),
     ("phc_sparse_table", c_i32, [c_vp, P(SystemC)]),
+    ("phc_sparse_evaluate", c_i32, [c_vp, P(c_dbl), P(c_dbl), P(c_dbl)]),
+    ("phc_sparse_evaluate_homogeneous", c_i32, [c_vp, P(c_dbl), P(c_dbl), P(c_dbl)]),
     ("phc_sparse_sample", c_i32, [c_vp, c_i32, P(c_i32), EVALUATOR, c_vp, c_i32, P(c_dbl)]),
     ("phc_homotopy_init", c_i32, [P(SystemC), c_i32, P(c_dbl), P(c_dbl), P(c_dbl),
                                   P(c_i64)]),

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <complex>
 #include <limits>
 #include <cstdlib>
 #include <cstring>
@@ -698,6 +699,70 @@ void phc_sparse_degrees(const phc_sparse* s, int32_t* d) {
   if (!s || !d) return;
   for (int i = 0; i < s->neq; ++i) d[i] = s->deg[i];
 }
+// sys%evaluate and sys%evaluate_homogeneous (src/sparse.f90:197-221) on the
+// host: f[neq] and jac (neq x m, column-major) of the table's terms at
+// v[m], m = n (affine: the exponents without the w column) or n + 1. A
+// term contributes c prod_l v_l^e_l to f_i and
+// c e_j v_j^(e_j - 1) prod_{l != j} v_l^e_l to jac(i, j), the products
+// taken over the nonzero exponents only, so zero coordinates need no
+// division and w = 0 is exact.
+namespace {
+using cdh = std::complex<double>;
+cdh powi(cdh x, int k) {  // x^k, k >= 0, square and multiply
+  cdh r = 1.0;
+  while (k > 0) {
+    if (k & 1) r *= x;
+    k >>= 1;
+    if (k) x *= x;
+  }
+  return r;
+}
+void eval_table(const phc_sparse* s, int m, const double* v, double* f, double* jac) {
+  const int n = s->n, neq = s->neq;
+  std::vector<cdh> z(m), F(neq, cdh(0.0)), J((size_t)neq * m, cdh(0.0));
+  for (int j = 0; j < m; ++j) z[j] = cdh(v[2 * j], v[2 * j + 1]);
+  for (int i = 0; i < neq; ++i)
+    for (int k = s->first[i]; k < s->first[i + 1]; ++k) {
+      const int32_t* e = &s->hexps[(size_t)k * (n + 1)];
+      const cdh c(s->coefs[2 * k], s->coefs[2 * k + 1]);
+      cdh val = c;
+      for (int l = 0; l < m; ++l)
+        if (e[l] > 0) val *= powi(z[l], e[l]);
+      F[i] += val;
+      for (int j = 0; j < m; ++j) {
+        if (e[j] <= 0) continue;
+        cdh d = c * (double)e[j] * powi(z[j], e[j] - 1);
+        for (int l = 0; l < m; ++l)
+          if (l != j && e[l] > 0) d *= powi(z[l], e[l]);
+        J[i + (size_t)j * neq] += d;
+      }
+    }
+  for (int i = 0; i < neq; ++i) {
+    f[2 * i] = F[i].real();
+    f[2 * i + 1] = F[i].imag();
+  }
+  for (size_t q = 0; q < J.size(); ++q) {
+    jac[2 * q] = J[q].real();
+    jac[2 * q + 1] = J[q].imag();
+  }
+}
+}  // namespace
+
+int32_t phc_sparse_evaluate(const phc_sparse* s, const double* x, double* f, double* jac) {
+  if (!s) return PHC_ERR_BAD_HANDLE;
+  if (!s->initialized || s->neq != s->n || !x || !f || !jac) return PHC_ERR_INVALID_INPUT;
+  eval_table(s, s->n, x, f, jac);
+  return PHC_OK;
+}
+
+int32_t phc_sparse_evaluate_homogeneous(const phc_sparse* s, const double* z, double* f,
+                                        double* jac) {
+  if (!s) return PHC_ERR_BAD_HANDLE;
+  if (!s->initialized || s->neq != s->n || !z || !f || !jac) return PHC_ERR_INVALID_INPUT;
+  eval_table(s, s->n + 1, z, f, jac);
+  return PHC_OK;
+}
+
 int32_t phc_sparse_table(const phc_sparse* s, phc_system* out) {
   if (!s || !out) return PHC_ERR_BAD_HANDLE;
   out->n = s->n;

@@ -199,10 +199,12 @@ int verify_plan(const unsigned char* bytes, size_t size) {
   if (bytes == nullptr || size < sizeof(PlanHeader)) return fail("short table");
   PlanHeader H;
   std::memcpy(&H, bytes, sizeof(H));
-  if (H.n < 1 || H.N != H.n + 1 || H.N > kMaxN) return fail("dimensions");
+  // (64-bit arithmetic throughout: a damaged header may hold any values)
+  if (H.n < 1 || (int64_t)H.N != (int64_t)H.n + 1 || H.N > kMaxN) return fail("dimensions");
   if (H.S < H.N || H.S % 2 == 0 || (int64_t)H.n * H.S > 1024) return fail("row stride");
-  if (H.maxexp < 1 || H.pw_size != (H.maxexp + 1) * H.N) return fail("power table size");
-  if (H.n_pre < 0 || H.pw_total != H.pw_size + H.n_pre || H.pw_total > kMaxPw)
+  if (H.maxexp < 1 || (int64_t)H.pw_size != ((int64_t)H.maxexp + 1) * H.N)
+    return fail("power table size");
+  if (H.n_pre < 0 || (int64_t)H.pw_total != (int64_t)H.pw_size + H.n_pre || H.pw_total > kMaxPw)
     return fail("extended power table size");
   if (H.n_levels < 0 || H.n_levels > kMaxLevels) return fail("levels");
   if (H.max_fac < 0 || H.max_fac > kMaxFac) return fail("factors per record");
@@ -223,6 +225,7 @@ int verify_plan(const unsigned char* bytes, size_t size) {
   for (int i = 0; i < H.n; ++i) {
     if (H.deg[i] < 1 || H.deg[i] - 1 > H.maxexp || H.radix[i] != radix) return fail("degrees");
     radix *= H.deg[i];
+    if (radix > (int64_t)INT32_MAX) return fail("path count");
   }
   if (H.nstart != radix) return fail("path count");
   // extended entries: level L may use plain entries and entries of levels < L

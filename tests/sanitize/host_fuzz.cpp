@@ -125,6 +125,14 @@ void fuzz_plan(const Sys& s) {
     return;
   }
   phc_homotopy h{{gamma[0], gamma[1]}, bb.data(), patch.data()};
+  // host evaluation of the table: F, F^h and their Jacobians at a random point
+  {
+    std::vector<double> z(2 * (s.n + 1)), f(2 * s.n), jac(2 * (size_t)s.n * (s.n + 1));
+    for (auto& v : z) v = normal();
+    CHECK(phc_sparse_evaluate(b, z.data(), f.data(), jac.data()) == PHC_OK);
+    CHECK(phc_sparse_evaluate_homogeneous(b, z.data(), f.data(), jac.data()) == PHC_OK);
+    for (double v : f) CHECK(std::isfinite(v));
+  }
   phc::HostPlan hp;
   const int st = phc::build_plan(&t, &h, &hp);
   CHECK(st == PHC_OK || st == PHC_ERR_UNSUPPORTED || st == PHC_ERR_INVALID_INPUT);
@@ -136,6 +144,14 @@ void fuzz_plan(const Sys& s) {
       std::vector<unsigned char> bad(hp.bytes);
       const size_t at = (size_t)uni(0, (int)bad.size() - 1);
       bad[at] ^= (unsigned char)(1u << uni(0, 7));
+      (void)phc::verify_plan(bad.data(), bad.size());
+    }
+    // header words overwritten with arbitrary values (sizes, offsets, counts)
+    for (int r = 0; r < 8; ++r) {
+      std::vector<unsigned char> bad(hp.bytes);
+      const size_t word = (size_t)uni(0, (int)(sizeof(phc::PlanHeader) / 4) - 1);
+      const uint32_t v = (uint32_t)rng();
+      std::memcpy(bad.data() + 4 * word, &v, 4);
       (void)phc::verify_plan(bad.data(), bad.size());
     }
     std::vector<unsigned char> shortened(hp.bytes.begin(), hp.bytes.begin() + hp.bytes.size() / 2);
