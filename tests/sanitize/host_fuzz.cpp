@@ -185,6 +185,18 @@ void fuzz_wire(const Sys& s) {
   CHECK(o2.seed == o.seed);
   ++n_wire;
   phc_sparse_destroy(d);
+  // requests with a 16- or 32-bit field overwritten by an arbitrary value
+  // (counts, sizes, exponents, variable indices): any status, no memory error
+  for (int r = 0; r < 16 && len >= 4; ++r) {
+    std::vector<unsigned char> bad(buf.begin(), buf.begin() + len);
+    const size_t at = (size_t)uni(0, (int)len - 4);
+    const uint32_t v = (uint32_t)rng();
+    std::memcpy(bad.data() + at, &v, uni(0, 1) ? 4 : 2);
+    phc_sparse* e = phc_sparse_create();
+    phc_solve_options o3;
+    (void)phc_request_decode(bad.data(), (int64_t)bad.size(), e, &o3);
+    phc_sparse_destroy(e);
+  }
   // damaged requests: any status, no memory error
   for (int r = 0; r < 16; ++r) {
     std::vector<unsigned char> bad(buf.begin(), buf.begin() + uni(0, (int)len));
