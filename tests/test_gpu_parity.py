@@ -158,13 +158,18 @@ def test_cfg2_parity_sample(orc):
         assert d.max() <= TOL_REGULAR
 
 
-@pytest.mark.parametrize("n", [16, 20, 28])
+@pytest.mark.parametrize("n", [16, 20, 28, 31])
 def test_wide_rows_parity_sample(orc, n):
     """Random sparse quadratic systems whose N = n+1 unknowns need the wider
     register rows (18, 24, 32 columns: the elimination without column-group
-    branches for 24 and 32, spilling kernels included); first 24 paths,
-    both precisions, against the restatement."""
+    branches for 24 and 32, spilling kernels included), up to the maximum
+    N = 32; first 24 paths, both precisions, against the restatement."""
     n_, eqs = W.sparse_quadratic(n, 24, W.seed_for(5, 100 + n))
+    if n == 31:
+        # 2^31 paths exceed the reference's integer bound (src/homotopy.f90:128-132):
+        # the last equation is linear, for 2^30 paths
+        g = W.Rng(W.seed_for(5, 231))
+        eqs[-1] = W.random_sparse(n, 1, 12, g)
     so = W.build(orc.SparseSystem, n_, eqs)
     sp = W.build(P.SparseSystem, n_, eqs)
     pr, zr, xr, st = orc.solve_paths(so, count=24, nthreads=8)
