@@ -4,8 +4,8 @@
  * Drop-in for the per-path work behind polyhomocont's
  *   subroutine solve(sys, res, status, options)       src/solve.f90:154-215
  * on type(sparse_system) inputs (src/sparse.f90:31-61). The Fortran side
- * keeps its API; a bind(C) interface packs the sparse
- * table and calls phc_solve_sparse, which:
+ * keeps its API; a bind(C) interface module on the Fortran side packs the
+ * sparse table and calls phc_solve_sparse, which:
  *   - seeds the reference generator and draws gamma, b, patch exactly as
  *     hom%init (src/homotopy.f90:104-149);
  *   - runs start_solution + endpoint + classify for every path on the GPU
@@ -282,19 +282,23 @@ int32_t phc_solve_paths(const phc_system* sys, const phc_homotopy* hom,
                         double* z_out, double* x_out);
 
 /* Per-path numerics without any device allocation. No counterpart in the
- * reference. For callers that cannot call cudaMalloc -- code that runs
- * inside CUDA graph capture, services whose device memory is reserved up
- * front, hosts that forbid device allocations after start-up. The caller
- * passes the host table and constants and its own device output buffers
- * (d_out[count], d_z[count][n+1][2], d_x[count][n][2] or NULL); the compiled
- * table and the path-queue counter go into one fixed 256 KiB array in device
- * memory that every GPU loading the library holds until exit. Tables larger
- * than that are rejected with PHC_ERR_UNSUPPORTED. The call only enqueues
- * work on `stream`; it calls no cudaMalloc, cudaFree or other allocating
- * routine. Its first call on a device looks up the array's address on that
- * device (make that first call before any stream capture). All calls share
- * the array: calls that overlap on the GPU (different streams, no ordering)
- * race on it; calls on one stream are ordered. */
+ * reference. For callers that cannot call cudaMalloc -- services whose
+ * device memory is reserved and accounted for up front, and hosts that
+ * forbid device allocations after start-up because an allocation can block
+ * or fail at an unpredictable moment. The caller passes the host table and
+ * constants and its own device output buffers (d_out[count],
+ * d_z[count][n+1][2], d_x[count][n][2] or NULL); the compiled table and the
+ * path-queue counter go into one fixed 256 KiB array in device memory that
+ * every GPU loading the library holds until exit. Tables larger than that
+ * are rejected with PHC_ERR_UNSUPPORTED. The call only enqueues work on
+ * `stream`; it calls no cudaMalloc, cudaFree or other allocating routine.
+ * Its first call on a device looks up the array's address on that device
+ * and caches it (make that first call before any stream capture; a
+ * cudaDeviceReset invalidates the cached address, so do not use the entry
+ * point on a device after one). All calls share the array, and each call
+ * rewrites the table and clears the queue counter it holds: calls that
+ * overlap on the GPU (different streams, no ordering) race on it; calls on
+ * one stream are ordered. */
 int32_t phc_solve_paths_noalloc(const phc_system* sys, const phc_homotopy* hom,
                                 const phc_solve_options* opts, const phc_gpu_options* gpu,
                                 int64_t k0, int64_t count, phc_path_out* d_out, double* d_z,

@@ -1,14 +1,20 @@
 // phc_noalloc.cu -- a tracker entry point that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc: code running inside a CUDA graph or
-// a capture region, memory-pool-managed services whose device memory is
-// accounted for up front, or hosts that forbid device allocations after
-// start-up. phc_solve_paths_noalloc serves them. The caller passes its
-// inputs (the system table and homotopy constants, in host memory) and its
-// outputs (device buffers it owns); the only other device memory the
-// tracker needs -- the compiled copy of the table and the path-queue
-// counter -- lives in the fixed-size array below, which every GPU that
-// loads the library holds until the process exits.
+// Some callers cannot call cudaMalloc: services whose device memory is
+// reserved and accounted for up front (a memory pool sized at start-up
+// that must not grow), and hosts whose policy forbids device allocations
+// after start-up because an allocation can block or fail at an
+// unpredictable moment. phc_solve_paths_noalloc serves them. The caller
+// passes its inputs (the system table and homotopy constants, in host
+// memory) and its outputs (device buffers it owns); the only other device
+// memory the tracker needs -- the compiled copy of the table and the
+// path-queue counter -- lives in the fixed-size array below, which every
+// GPU that loads the library holds until the process exits.
+//
+// The array's device address is looked up on the first call on each
+// device and cached; a cudaDeviceReset (or anything else that destroys the
+// device's primary context) invalidates the cached address, so the entry
+// point must not be used on a device after such a reset.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -64,7 +70,8 @@ extern "C" int32_t phc_solve_paths_noalloc(const phc_system* sys, const phc_homo
   HostPlan hp;
   st = build_plan(sys, hom, &hp);
   if (st != PHC_OK) return st;
-  if (k0 + count - 1 > hp.nstart) return PHC_ERR_INVALID_INPUT;
+  // k0 + count - 1 <= nstart, written so that no sum can overflow
+  if (k0 - 1 > hp.nstart - count) return PHC_ERR_INVALID_INPUT;
   if (hp.bytes.size() > kNoAllocBytes - kTableOffset) {
     set_last_error("system table larger than the no-alloc scratch array (256 KiB); "
                    "use phc_solve_paths or phc_plan_create");
@@ -80,7 +87,9 @@ extern "C" int32_t phc_solve_paths_noalloc(const phc_system* sys, const phc_homo
   st = resolve_launch(hp, g, g.device, &cfg);
   if (st != PHC_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // the counter must start at zero; the table is rewritten by every call
+  // the counter must start at zero; the table is rewritten by every call.
+  // hp.bytes is pageable host memory: the copy has been staged by the time
+  // cudaMemcpyAsync returns, so the buffer may be freed when this call ends.
   e = cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(no-alloc counter)");
   e = cudaMemcpyAsync(scratch + kTableOffset, hp.bytes.data(), hp.bytes.size(),
@@ -89,7 +98,7 @@ extern "C" int32_t phc_solve_paths_noalloc(const phc_system* sys, const phc_homo
   KParams kp;
   std::memset(&kp, 0, sizeof(kp));
   kp.plan = scratch + kTableOffset;
-  kp.plan_bytes = align16((int)hp.bytes.size());
+  kp.plan_bytes = cfg.plan_bytes;
   kp.ws_bytes = cfg.ws_bytes;
   kp.warps = cfg.warps;
   kp.persistent = cfg.persistent;
