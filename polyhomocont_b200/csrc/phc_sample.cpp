@@ -39,7 +39,9 @@
 #include <cstdint>
 #include <condition_variable>
 #include <map>
+#include <memory>
 #include <mutex>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -146,8 +148,8 @@ bool least_squares(std::vector<cd>& A, int rows, int cols, std::vector<cd>& B, i
   double dmax = 0.0, vv = 0.0;
   bool failed = false;
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const int T = cols >= 192 ? (int)std::min(hw, 16u) : 1;
-  Barrier bar(T);
+  int T = cols >= 192 ? (int)std::min(hw, 16u) : 1;
+  std::unique_ptr<Barrier> bar;
   auto work = [&](int t) {
     for (int k = 0; k < cols; ++k) {
       cd* a = &A[(size_t)k * rows];
@@ -167,7 +169,7 @@ bool least_squares(std::vector<cd>& A, int rows, int cols, std::vector<cd>& B, i
           dmax = std::max(dmax, s);
         }
       }
-      if (T > 1) bar.wait();
+      if (T > 1) bar->wait();
       if (failed) return;
       // columns k+1 .. cols-1, then the right-hand sides, in T contiguous ranges
       const int rest = cols - k - 1, m = rest + nrhs;
@@ -179,17 +181,50 @@ bool least_squares(std::vector<cd>& A, int rows, int cols, std::vector<cd>& B, i
         const cd f = 2.0 * dot / vv;
         for (int i = k; i < rows; ++i) y[i] -= f * a[i];
       }
-      if (T > 1) bar.wait();
+      if (T > 1) bar->wait();
     }
   };
-  if (T == 1) {
-    work(0);
-  } else {
-    std::vector<std::thread> pool;
-    for (int t = 1; t < T; ++t) pool.emplace_back(work, t);
-    work(0);
-    for (auto& th : pool) th.join();
+  // Helper threads wait at a gate until the whole pool exists. If a thread
+  // cannot be created (std::system_error), the gate tells the ones already
+  // started to return, and the factorization runs on this thread alone.
+  std::vector<std::thread> pool;
+  std::mutex gate_mu;
+  std::condition_variable gate_cv;
+  int gate = T > 1 ? 0 : 1;  // 0 closed, 1 run, 2 abandon
+  bool pool_ok = true;
+  try {
+    for (int t = 1; t < T; ++t)
+      pool.emplace_back([&, t] {
+        {
+          std::unique_lock<std::mutex> lk(gate_mu);
+          gate_cv.wait(lk, [&] { return gate != 0; });
+          if (gate == 2) return;
+        }
+        work(t);
+      });
+  } catch (const std::system_error&) {
+    pool_ok = false;
   }
+  if (!pool_ok) {
+    {
+      std::lock_guard<std::mutex> lk(gate_mu);
+      gate = 2;
+    }
+    gate_cv.notify_all();
+    for (auto& th : pool) th.join();
+    pool.clear();
+    T = 1;
+  }
+  bar.reset(new Barrier(T));
+  if (T > 1) {
+    {
+      std::lock_guard<std::mutex> lk(gate_mu);
+      gate = 1;
+    }
+    gate_cv.notify_all();
+  }
+  work(0);
+  for (auto& th : pool) th.join();
   if (failed) return false;
   for (int k = 0; k < cols; ++k)
     if (std::abs(diag[k]) <= 1e-10 * dmax) return false;
