@@ -213,11 +213,15 @@ int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, Lau
   int tw = 4, tc = 1;
   tuned_launch(device, cfg->precision, cfg->persistent, cfg->nm, &tw, &tc);
   cfg->chunk = g.chunk > 0 ? g.chunk : tc;
-  cfg->ws_bytes = ws_layout(hp.n, hp.S, hp.pw_size, cfg->precision == PHC_PREC_MIXED).bytes;
-  const int plan_bytes = align16((int)hp.bytes.size());
+  cfg->eval32 = kernel_eval32(cfg->nm, cfg->precision) ? 1 : 0;
+  cfg->ws_bytes = ws_layout(hp.n, hp.S, hp.pw_size, cfg->eval32 != 0).bytes;
+  // kernels without the FP32 evaluation stage the table without its FP32
+  // coefficients
+  const int plan_bytes = cfg->eval32 ? align16((int)hp.bytes.size()) : hp.bytes_fp64;
+  cfg->plan_bytes = plan_bytes;
   const int smax = device_smem_optin(device);
   int warps = g.warps_per_block > 0 ? g.warps_per_block : tw;
-  warps = std::min(std::max(warps, 1), 8);
+  warps = std::min(std::max(warps, 1), max_warps_per_block(cfg->nm));
   while (warps > 1 && plan_bytes + warps * cfg->ws_bytes > smax) --warps;
   if (plan_bytes + warps * cfg->ws_bytes > smax) {
     set_last_error("system table does not fit in shared memory");
@@ -315,7 +319,7 @@ static int run_paths_sync(const HostPlan& hp, const phc_solve_options& so,
   KParams kp;
   std::memset(&kp, 0, sizeof(kp));
   kp.plan = static_cast<const unsigned char*>(W.plan.p);
-  kp.plan_bytes = align16((int)hp.bytes.size());
+  kp.plan_bytes = cfg.plan_bytes;
   kp.ws_bytes = cfg.ws_bytes;
   kp.warps = cfg.warps;
   kp.persistent = cfg.persistent;
@@ -814,7 +818,7 @@ int32_t phc_solve_paths(const phc_system* sys, const phc_homotopy* hom,
   HostPlan hp;
   st = build_plan(sys, hom, &hp);
   if (st != PHC_OK) return st;
-  if (k0 + count - 1 > hp.nstart) return PHC_ERR_INVALID_INPUT;
+  if (k0 - 1 > hp.nstart - count) return PHC_ERR_INVALID_INPUT;  // k0 + count - 1 <= nstart
   return run_paths_sync(hp, so, g, k0, count, out, z_out, x_out);
 }
 
@@ -910,13 +914,14 @@ int32_t phc_plan_launch(phc_plan* p, int64_t k0, int64_t count, phc_path_out* d_
                         double* d_z, void* stream) {
   if (!p) return PHC_ERR_BAD_HANDLE;
   if (count <= 0) return PHC_OK;
-  if (k0 < 1 || k0 + count - 1 > p->hp.nstart || !d_out || !d_z) return PHC_ERR_INVALID_INPUT;
+  if (k0 < 1 || k0 - 1 > p->hp.nstart - count || !d_out || !d_z)
+    return PHC_ERR_INVALID_INPUT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   PHC_CUDA(cudaSetDevice(p->device));
   KParams kp;
   std::memset(&kp, 0, sizeof(kp));
   kp.plan = static_cast<const unsigned char*>(p->d_plan);
-  kp.plan_bytes = align16((int)p->hp.bytes.size());
+  kp.plan_bytes = p->cfg.plan_bytes;
   kp.ws_bytes = p->cfg.ws_bytes;
   kp.warps = p->cfg.warps;
   kp.persistent = p->cfg.persistent;
@@ -957,7 +962,8 @@ int32_t phc_graph_create(phc_plan* p, int64_t k0, int64_t count, phc_path_out* d
                          double* d_z, phc_graph** out) {
   if (!p || !out) return PHC_ERR_BAD_HANDLE;
   *out = nullptr;
-  if (count <= 0 || k0 < 1 || k0 + count - 1 > p->hp.nstart || !d_out || !d_z)
+  if (count <= 0 || k0 < 1 || k0 - 1 > p->hp.nstart - count || !d_out ||
+      !d_z)
     return PHC_ERR_INVALID_INPUT;
   PHC_CUDA(cudaSetDevice(p->device));
   std::unique_ptr<phc_graph> g(new (std::nothrow) phc_graph());

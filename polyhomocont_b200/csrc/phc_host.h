@@ -18,6 +18,7 @@ struct HostPlan {
   std::vector<unsigned char> bytes;  // PlanHeader + records
   int n = 0, N = 0, S = 0, maxexp = 0, pw_size = 0, nrec = 0;
   int max_fac = 0;  // most power-table factors of a Jacobian record
+  int bytes_fp64 = 0;  // leading bytes without the FP32 coefficients
   int64_t nstart = 0;
 };
 
@@ -53,6 +54,8 @@ struct LaunchCfg {
   int persistent = 0;
   int chunk = 1;
   int grid = 0;        // persistent grid (blocks)
+  int eval32 = 0;      // the kernel carries the FP32 evaluation
+  int plan_bytes = 0;  // table bytes the kernel stages into shared memory
   int ws_bytes = 0;
   int smem = 0;        // dynamic shared memory per block
 };

@@ -47,7 +47,9 @@ constexpr int kMaxLevels = 8;
 // Records are stored lane-interleaved: record i of lane l sits in slot
 // i * 32 + l of three arrays (FP64 coefficient, FP32 coefficient, metadata),
 // so the 32 lanes of a warp read consecutive 16-, 8- and 8-byte words
-// without shared-memory bank conflicts.
+// without shared-memory bank conflicts. The FP32 coefficient arrays are the
+// table's last bytes, so that kernels that evaluate only in FP64 stage the
+// first bytes_fp64 bytes and leave them out.
 struct alignas(16) PlanHeader {
   int32_t n;            // variables / equations
   int32_t N;            // unknowns n + 1
@@ -66,7 +68,8 @@ struct alignas(16) PlanHeader {
   int32_t level_off[kMaxLevels + 1];  // word ranges per level (2 words per entry)
   int32_t pw_total;     // pw_size + n_pre: entries of the per-warp table
   int32_t max_fac;      // most power-table factors of any Jacobian record (0..3)
-  int32_t pad0_;
+  int32_t bytes_fp64;   // bytes before the FP32 coefficient arrays (which come last):
+                        // what a kernel without an FP32 evaluation stages
   int32_t cnt_f[kWarp]; // records of each lane
   int32_t cnt_j[kWarp];
   int32_t deg[kMaxN];
@@ -145,6 +148,9 @@ struct KParamsBatch {
 // (one per warp) so that registers stay free for the evaluation and the LU.
 // Scalars are warp-uniform; the vectors hold component j in slot j.
 struct alignas(16) WarpState {
+  // the path: its current point z, the segment's start point zs, the
+  // corrector's point zp, the RK4 sum, the pending unit's input point zin
+  double z[kWarp][2], zs[kWarp][2], zp[kWarp][2], ksum[kWarp][2], zin[kWarp][2];
   double zold[kWarp][2];   // end game: z before a radial segment
   double est[kWarp][2];    // current Cauchy estimate
   double prev[kWarp][2];   // previous estimate
@@ -161,7 +167,17 @@ struct alignas(16) WarpState {
       eg_radius, rec_err;
   double lp_spacing, lp_floor, lp_dth;
   double cond_anorm, cond_ainv;  // cond1 accumulated over right-hand-side chunks
+  // segment stepper (track_segment's s, step, ds, s + ds, Newton's last
+  // squared update norm) and the pending unit's t and dt/ds
+  double s, step, ds, sn, dnorm_prev;
+  double tin[2], dtin[2];
   long long units;
+  long long kpath;               // the path (1-based)
+  phc_path_out* rec;             // its outputs
+  double* zo;
+  double* xo;
+  int nsucc, sacc, srej, sstat;  // segment: accepted since the last growth, counts, status
+  int stage, att64, uk, pc_after, u_prec;  // RK4 stage / Newton iteration; pending unit
   int seg_arc, o_grow, seg_cont;
   int p_status, p_wind, p_egs, p_nacc, p_nrej, p_atinf, p_sing, p_real;
   int c_tan, c_new, c_ref, c_eval, c_cond, c_retry;
@@ -179,13 +195,15 @@ struct WsLayout {
 
 PHC_HD inline int align16(int x) { return (x + 15) & ~15; }
 
-PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size, bool mixed) {
+// eval32: the kernel carries the FP32 evaluation (FP32 power table and
+// Jacobian buffer).
+PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size, bool eval32) {
   WsLayout L;
   int off = 0;
   L.pwd = off; off += align16(pw_size * 16);
-  L.pwf = off; off += mixed ? align16(pw_size * 8) : 0;
+  L.pwf = off; off += eval32 ? align16(pw_size * 8) : 0;
   L.jd = off; off += align16((n + 1) * S * 16);  // rows 0..n-1: dF^h, row n: patch
-  L.jf = off; off += mixed ? align16((n + 1) * S * 8) : 0;
+  L.jf = off; off += eval32 ? align16((n + 1) * S * 8) : 0;
   L.piv = off; off += kWarp * 4;
   L.st = off; off += align16((int)sizeof(WarpState));
   L.bytes = off;
@@ -199,5 +217,17 @@ inline int pick_nm(int N) {
     if (N <= v) return v;
   return 0;
 }
+// The single-system kernels of rows up to 8 columns carry an FP32
+// evaluation for the mixed predictor; every other kernel evaluates in FP64.
+PHC_HD constexpr bool kernel_eval32(int nm, int precision) {
+  return precision == PHC_PREC_MIXED && nm <= 8;
+}
+// Most warps per block of the tracking kernels. Rows of up to 18 columns
+// are compiled for blocks of up to 12 warps, so that 12 warps share one
+// staged copy of the table; that bounds their registers at 65,536 / 384 =
+// 170 per thread, which they fit without spilling. The wider rows need more
+// registers and are compiled for blocks of up to 8 warps (255 registers).
+PHC_HD constexpr int max_warps_per_block(int nm) { return nm <= 18 ? 12 : 8; }
+constexpr int kMaxWarpsPerBlock = 12;  // over all row widths
 
 }  // namespace phc

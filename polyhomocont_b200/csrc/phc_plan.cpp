@@ -221,6 +221,16 @@ int verify_plan(const unsigned char* bytes, size_t size) {
       !region(H.off_jd, sj * 16) || !region(H.off_jf, sj * 8) || !region(H.off_jm, sj * 8) ||
       !region(H.off_pre, (int64_t)H.n_pre * 8))
     return fail("array offsets");
+  // kernels that evaluate only in FP64 stage the first bytes_fp64 bytes:
+  // everything but the FP32 coefficients must lie there
+  auto region64 = [&](int32_t off, int64_t bytes_needed) {
+    return (int64_t)off + bytes_needed <= (int64_t)H.bytes_fp64;
+  };
+  if (H.bytes_fp64 < (int)sizeof(PlanHeader) || H.bytes_fp64 % 16 ||
+      H.bytes_fp64 > H.total_bytes || !region64(H.off_fd, sf * 16) ||
+      !region64(H.off_fm, sf * 8) || !region64(H.off_jd, sj * 16) ||
+      !region64(H.off_jm, sj * 8) || !region64(H.off_pre, (int64_t)H.n_pre * 8))
+    return fail("FP64 part of the table");
   int64_t radix = 1;
   for (int i = 0; i < H.n; ++i) {
     if (H.deg[i] < 1 || H.deg[i] - 1 > H.maxexp || H.radix[i] != radix) return fail("degrees");
@@ -430,12 +440,15 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   };
   const size_t sf = (size_t)len_f * kWarp, sj = (size_t)len_j * kWarp;
   H.off_fd = take(sf * 16);
-  H.off_ff = take(sf * 8);
   H.off_fm = take(sf * 8);
   H.off_jd = take(sj * 16);
-  H.off_jf = take(sj * 8);
   H.off_jm = take(sj * 8);
   H.off_pre = take(pre_packed.size() * 4);
+  // the FP32 coefficients last: kernels that evaluate only in FP64 stage
+  // the table without them
+  H.bytes_fp64 = (int32_t)off;
+  H.off_ff = take(sf * 8);
+  H.off_jf = take(sj * 8);
   H.total_bytes = (int32_t)off;
   int nrec = 0;
   for (const auto& v : lf) nrec += (int)v.size();
@@ -455,6 +468,7 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   out->nstart = radix;
   out->nrec = nrec;
   out->max_fac = max_fac;
+  out->bytes_fp64 = H.bytes_fp64;
   return verify_plan(out->bytes.data(), out->bytes.size());
 }
 

@@ -180,7 +180,9 @@ int launch_batch(phc_server* S, Slot& s) {
   size_t plan_end = up256(s.batch.size() * sizeof(BatchSys));
   for (size_t i = 0; i < s.batch.size(); ++i) {
     Request& r = *s.batch[i];
-    const int tb = align16((int)r.plan.bytes.size());
+    // the batch kernels evaluate in FP64 only: their warps stage the table
+    // without its FP32 coefficients
+    const int tb = r.plan.bytes_fp64;
     std::memcpy(s.hbuf + r.off_plan, r.plan.bytes.data(), r.plan.bytes.size());
     plan_end = std::max(plan_end, r.off_plan + up256(r.plan.bytes.size()));
     std::memset(&d[i], 0, sizeof(BatchSys));
@@ -196,11 +198,13 @@ int launch_batch(phc_server* S, Slot& s) {
     nm = std::max(nm, r.cfg.nm);
     fac = std::max(fac, r.cfg.fac);
     table_cap = std::max(table_cap, tb);
-    ws_cap = std::max(ws_cap, align16(r.cfg.ws_bytes));
+    ws_cap = std::max(ws_cap, ws_layout(r.plan.n, r.plan.S, r.plan.pw_size, false).bytes);
   }
   const int slice = table_cap + ws_cap + align16((int)sizeof(KOpts));
   const int smax = device_smem_optin(S->cfg.device);
-  int warps = g.warps_per_block > 0 ? std::min(std::max(g.warps_per_block, 1), 8) : 4;
+  int warps = g.warps_per_block > 0
+                  ? std::min(std::max(g.warps_per_block, 1), max_warps_per_block(nm))
+                  : 4;
   while (warps > 1 && warps * slice > smax) --warps;
   if (warps * slice > smax) {
     set_last_error("batch tables do not fit in shared memory");

@@ -62,6 +62,25 @@ constexpr int kCondChunk = 4;
 // Rows of up to 16 columns use the split layout (two lanes per row, half
 // a row each: evaluate_split, gauss_jordan_split); wider rows one lane per
 // row.
+// Workspace pointers of a warp inside its shared-memory region. The FP32
+// power table and Jacobian buffer exist only in kernels that carry the FP32
+// evaluation (EVAL32).
+template <bool EVAL32>
+__device__ __forceinline__ WarpWS warp_workspace(const PlanHeader& P, unsigned char* wbase) {
+  const WsLayout L = ws_layout(P.n, P.S, P.pw_total, EVAL32);
+  WarpWS ws;
+  ws.pwd = reinterpret_cast<cd*>(wbase + L.pwd);
+  ws.pwf = reinterpret_cast<cf*>(wbase + L.pwf);
+  ws.jd = reinterpret_cast<cd*>(wbase + L.jd);
+  ws.jf = reinterpret_cast<cf*>(wbase + L.jf);
+  ws.piv = reinterpret_cast<int*>(wbase + L.piv);
+  return ws;
+}
+template <bool EVAL32>
+__device__ __forceinline__ WarpState* warp_state(const PlanHeader& P, unsigned char* wbase) {
+  return reinterpret_cast<WarpState*>(wbase + ws_layout(P.n, P.S, P.pw_total, EVAL32).st);
+}
+
 template <int NM>
 struct RowLayout {
   static constexpr int kLanes = NM <= 8 ? 4 : (NM <= 16 ? 2 : 1);  // lanes per row
@@ -91,11 +110,19 @@ __device__ __forceinline__ bool eliminate(cpx<T> (&a)[RowLayout<NM>::kRegs], cpx
     return gauss_jordan<NM, R, T>(a, r, N, lane, piv);
 }
 
+// The unit reads the system's constants and its workspace pointers from
+// shared memory itself (tbl: the staged table, wbase: the warp's
+// workspace), so that nothing of them stays live in registers between
+// units.
 template <int NM, bool MIXED, bool EVAL32, int F>
-__device__ __forceinline__ void run_unit(const WarpConst& C, const WarpWS& ws, int kind, int prec,
-                                         int c0, cd zin, cd t, cd dt, int lane, UnitRes& u) {
+__device__ __forceinline__ void run_unit(const unsigned char* tbl, unsigned char* wbase, int kind,
+                                         int prec, int c0, cd zin, cd t, cd dt, int lane,
+                                         UnitRes& u) {
   using L = RowLayout<NM>;
   constexpr int RW = L::kRegs;
+  const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(tbl);
+  const WarpConst C = load_warp_const(P, tbl, lane);
+  const WarpWS ws = warp_workspace<EVAL32>(P, wbase);
   const int N = C.N;
   // the row this lane works on, and whether it reports it (one lane per row)
   const int row = lane & (L::kRows - 1);
@@ -254,6 +281,16 @@ __device__ __forceinline__ void seg_tdt(const WarpState& st, double s, cd& t, cd
   dt = mkc<double>(0.0, st.seg_dth) * t;
 }
 
+// t(s) and dt/ds into the warp state (the pending unit's t and dt)
+__device__ __forceinline__ void seg_tdt_store(WarpState& st, double s) {
+  cd t, dt;
+  seg_tdt(st, s, t, dt);
+  st.tin[0] = t.re;
+  st.tin[1] = t.im;
+  st.dtin[0] = dt.re;
+  st.dtin[1] = dt.im;
+}
+
 // max_j |v_j|^2 over the warp (squared moduli compare like the moduli of
 // the reference's norm_inf, without a hypot per lane)
 __device__ __forceinline__ double vnorm2(cd v, int lane, int N) {
@@ -265,32 +302,31 @@ __device__ __forceinline__ double vnorm2(cd v, int lane, int N) {
 #define STV(f, v) sts(&LV(f), (v))
 
 // Tracks path k (1-based) and writes its record, z and x.
+//
+// The state of the path -- the lane vectors z, the segment's start point
+// zs, the prediction zp and the RK4 sum, the segment stepper's scalars, the
+// pending unit's inputs -- lives in the warp's WarpState in shared memory,
+// not in registers: the state machine touches it a few times per unit,
+// while the unit (an evaluation and an elimination, thousands of
+// instructions) then has the register file to itself. Only the control
+// state pc and the unit's result U stay in registers across a unit.
 template <int NM, int PREC, bool EVAL32, int F>
-__device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& C,
-                                          const WarpWS& ws, WarpState& st, const KOpts& O,
-                                          int64_t k, int lane, phc_path_out* rec, double* zo,
-                                          double* xo) {
+__device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned char* wbase,
+                                          WarpState& st, const KOpts& O, int64_t k, int lane,
+                                          phc_path_out* rec, double* zo, double* xo) {
   const phc_tracker_options& TO = O.so.tracker;
   const phc_endgame_options& EO = O.so.endgame;
-  const int n = C.n, N = C.N;
   constexpr bool kMixed = (PREC == PHC_PREC_MIXED);
-
-  // hot lane vectors (component j in lane j)
-  cd z = czero<double>(), zs = z, zp = z, ksum = z, zin = z;
-  // hot uniform state of the segment being tracked
-  double s = 0.0, step = 0.0, ds = 0.0, sn = 0.0, dnorm_prev = kHuge;
-  int nsucc = 0, sacc = 0, srej = 0, sstat = PHC_PATH_SUCCESS, stage = 0;
-  bool att64 = true;
-  // pending unit
-  int uk = UK_TANGENT, pc_after = PC_FINISH;
-  int u_prec = 0;  // 0: FP64, 1: FP64 evaluation + FP32 elimination, 2: FP32 evaluation + elimination
-  cd tin = z, dtin = z;
   UnitRes U;
   U.x = U.h = czero<double>();
   U.a1 = U.a2 = 0.0;
   U.ok = true;
 
   // path result defaults (type(path_result), src/solve.f90:86-119)
+  st.kpath = k;
+  st.rec = rec;
+  st.zo = zo;
+  st.xo = xo;
   st.p_status = PHC_PATH_SUCCESS;
   st.p_wind = st.p_egs = st.p_nacc = st.p_nrej = 0;
   st.p_t = 1.0;
@@ -300,18 +336,23 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
   st.units = 0;
   st.sticky = 0;
   st.cond_c0 = 0;
+  st.dnorm_prev = kHuge;
   STV(xv, czero<double>());
 
   int pc = PC_START;
   for (;;) {
     bool want = false;
     while (!want) {
+      const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(tbl);
+      const int n = P.n, N = P.N;
       switch (pc) {
         case PC_START: {
           // tdh_start_solution, src/homotopy.f90:151-177
+          const int64_t kk = st.kpath;
+          cd z = czero<double>();
           if (lane < n) {
             const int d = P.deg[lane];
-            const int64_t digit = ((k - 1) / P.radix[lane]) % d;
+            const int64_t digit = ((kk - 1) / P.radix[lane]) % d;
             const double phi = (P.argb[lane] + 2.0 * kPi * (double)digit) / (double)d;
             double sp, cp;
             sincos(phi, &sp, &cp);
@@ -323,6 +364,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
                                    : czero<double>();
           const cd sum = warp_csum(pz);
           if (lane < N) z = cdiv(z, sum);
+          STV(z, z);
           // track_path(hom, z, 1, t_end), src/solve.f90:230-232
           st.seg_arc = 0;
           st.seg_t0[0] = 1.0;
@@ -332,7 +374,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           st.o_step_init = TO.step_init;
           st.o_step_max = TO.step_max;
           st.o_grow = TO.grow_after;
-          zs = z;
+          STV(zs, z);
           st.seg_cont = PC_MAIN_DONE;
           pc = PC_SEG_BEGIN;
           break;
@@ -340,86 +382,98 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
 
         // ---------------- track_segment, src/tracker.f90:196-264 -------------
         case PC_SEG_BEGIN:
-          s = 0.0;
-          step = fmin(st.o_step_init, st.o_step_max);
-          nsucc = 0;
-          sacc = 0;
-          srej = 0;
-          sstat = PHC_PATH_SUCCESS;
+          st.s = 0.0;
+          st.step = fmin(st.o_step_init, st.o_step_max);
+          st.nsucc = 0;
+          st.sacc = 0;
+          st.srej = 0;
+          st.sstat = PHC_PATH_SUCCESS;
           pc = PC_SEG_ATTEMPT;
           break;
 
         case PC_SEG_ATTEMPT: {
+          const double s = st.s, step = st.step;
           if (!(s < 1.0)) {
             pc = PC_SEG_END;
             break;
           }
-          if (sacc + srej >= TO.max_steps || st.units > O.max_units) {
-            sstat = PHC_PATH_FAILED_MAX_STEPS;
+          if (st.sacc + st.srej >= TO.max_steps || st.units > O.max_units) {
+            st.sstat = PHC_PATH_FAILED_MAX_STEPS;
             pc = PC_SEG_END;
             break;
           }
-          ds = fmin(step, 1.0 - s);
-          sn = s + ds;
+          double ds = fmin(step, 1.0 - s);
+          double sn = s + ds;
           if (1.0 - sn <= 1.0e-3 * step) {
             sn = 1.0;
             ds = 1.0 - s;
           }
+          st.ds = ds;
+          st.sn = sn;
           const int sticky = st.sticky;
-          att64 = !kMixed || sticky > 0;
+          const bool att64 = !kMixed || sticky > 0;
+          st.att64 = att64 ? 1 : 0;
           if (sticky > 0) st.sticky = sticky - 1;
           // predict_rk4 stage 1: tangent at (z, s), src/tracker.f90:283
-          stage = 0;
-          uk = UK_TANGENT;
-          u_prec = att64 ? 0 : (EVAL32 ? 2 : 1);
-          zin = zs;
-          seg_tdt(st, s, tin, dtin);
-          pc_after = PC_SEG_AFTER_UNIT;
+          st.stage = 0;
+          st.uk = UK_TANGENT;
+          st.u_prec = att64 ? 0 : (EVAL32 ? 2 : 1);
+          STV(zin, LDV(zs));
+          seg_tdt_store(st, s);
+          st.pc_after = PC_SEG_AFTER_UNIT;
           want = true;
           break;
         }
 
         case PC_SEG_AFTER_UNIT: {
           int outcome = 0;  // 1 accept, 2 reject
+          const int stage = st.stage;
           if (stage < 4) {
             ++st.c_tan;
             if (!U.ok) {
               outcome = 2;
             } else {
               // predict_rk4, src/tracker.f90:266-293
+              const double s = st.s, ds = st.ds;
               const cd kk = U.x;
+              const cd zs = LDV(zs);
               double s_in = s;
               if (stage == 0) {
-                ksum = kk;
-                zin = zs + (0.5 * ds) * kk;
+                STV(ksum, kk);
+                STV(zin, zs + (0.5 * ds) * kk);
                 s_in = s + 0.5 * ds;
               } else if (stage == 1) {
-                ksum = ksum + 2.0 * kk;
-                zin = zs + (0.5 * ds) * kk;
+                STV(ksum, LDV(ksum) + 2.0 * kk);
+                STV(zin, zs + (0.5 * ds) * kk);
                 s_in = s + 0.5 * ds;
               } else if (stage == 2) {
-                ksum = ksum + 2.0 * kk;
-                zin = zs + ds * kk;
+                STV(ksum, LDV(ksum) + 2.0 * kk);
+                STV(zin, zs + ds * kk);
                 s_in = s + ds;
               } else {
-                ksum = ksum + kk;
-                zp = zs + (ds / 6.0) * ksum;
+                const cd ksum = LDV(ksum) + kk;
+                STV(zp, zs + (ds / 6.0) * ksum);
               }
               if (stage < 3) {
-                ++stage;
-                uk = UK_TANGENT;
+                st.stage = stage + 1;
+                st.uk = UK_TANGENT;
                 // stages 1 and 2 share s + ds/2: t and dt/ds are reused
-                if (stage != 2) seg_tdt(st, s_in, tin, dtin);
+                if (stage + 1 != 2) seg_tdt_store(st, s_in);
               } else {
                 // newton_correct at t(sn), src/tracker.f90:319-360
-                stage = 4;
-                dnorm_prev = kHuge;
-                uk = UK_NEWTON;
-                u_prec = att64 ? 0 : 1;
-                zin = zp;
-                if (sn != s + ds) tin = seg_t(st, sn);  // else t(s + ds) of stage 3
+                st.stage = 4;
+                st.dnorm_prev = kHuge;
+                st.uk = UK_NEWTON;
+                st.u_prec = st.att64 ? 0 : 1;
+                STV(zin, LDV(zp));
+                const double sn = st.sn;
+                if (sn != s + ds) {  // else t(s + ds) of stage 3
+                  const cd t = seg_t(st, sn);
+                  st.tin[0] = t.re;
+                  st.tin[1] = t.im;
+                }
               }
-              pc_after = PC_SEG_AFTER_UNIT;
+              st.pc_after = PC_SEG_AFTER_UNIT;
               want = true;
               break;
             }
@@ -429,23 +483,24 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
             if (!U.ok) {
               outcome = 2;
             } else {
-              zp = zp + U.x;
+              const cd zp = LDV(zp) + U.x;
+              STV(zp, zp);
               // ||dz|| <= tol ||z|| and the contraction test on squared norms
               const double d2 = vnorm2(U.x, lane, N);
               const double z2 = vnorm2(zp, lane, N);
               if (d2 <= (TO.corrector_tol * TO.corrector_tol) * z2) {
                 outcome = 1;
-              } else if (it > 1 && d2 > (TO.contraction * TO.contraction) * dnorm_prev) {
+              } else if (it > 1 && d2 > (TO.contraction * TO.contraction) * st.dnorm_prev) {
                 outcome = 2;
               } else {
-                dnorm_prev = d2;
+                st.dnorm_prev = d2;
                 if (it >= TO.corrector_maxit) {
                   outcome = 2;
                 } else {
-                  ++stage;
-                  uk = UK_NEWTON;
-                  zin = zp;
-                  pc_after = PC_SEG_AFTER_UNIT;
+                  st.stage = stage + 1;
+                  st.uk = UK_NEWTON;
+                  STV(zin, zp);
+                  st.pc_after = PC_SEG_AFTER_UNIT;
                   want = true;
                   break;
                 }
@@ -453,35 +508,38 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
             }
           }
           if (outcome == 1) {
-            zs = zp;
-            s = sn;
-            ++sacc;
-            ++nsucc;
+            STV(zs, LDV(zp));
+            st.s = st.sn;
+            ++st.sacc;
+            const int nsucc = st.nsucc + 1;
             if (nsucc >= st.o_grow) {
-              step = fmin(2.0 * step, st.o_step_max);
-              nsucc = 0;
+              st.step = fmin(2.0 * st.step, st.o_step_max);
+              st.nsucc = 0;
+            } else {
+              st.nsucc = nsucc;
             }
             pc = PC_SEG_ATTEMPT;
           } else {
-            if (kMixed && !att64) {
+            if (kMixed && !st.att64) {
               // the FP32 attempt failed: redo the same step in FP64 before
               // counting a rejection, and stay in FP64 for a few steps
-              att64 = true;
+              st.att64 = 1;
               st.sticky = O.fp64_sticky;
-              stage = 0;
-              uk = UK_TANGENT;
-              u_prec = 0;
-              zin = zs;
-              seg_tdt(st, s, tin, dtin);
-              pc_after = PC_SEG_AFTER_UNIT;
+              st.stage = 0;
+              st.uk = UK_TANGENT;
+              st.u_prec = 0;
+              STV(zin, LDV(zs));
+              seg_tdt_store(st, st.s);
+              st.pc_after = PC_SEG_AFTER_UNIT;
               want = true;
               break;
             }
-            ++srej;
-            nsucc = 0;
-            step = 0.5 * step;
+            ++st.srej;
+            st.nsucc = 0;
+            const double step = 0.5 * st.step;
+            st.step = step;
             if (step < TO.step_min) {
-              sstat = PHC_PATH_FAILED_MIN_STEP;
+              st.sstat = PHC_PATH_FAILED_MIN_STEP;
               pc = PC_SEG_END;
             } else {
               pc = PC_SEG_ATTEMPT;
@@ -495,12 +553,13 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           break;
 
         // ---------------- endpoint, src/solve.f90:217-252 ----------------------
-        case PC_MAIN_DONE:
-          z = zs;
+        case PC_MAIN_DONE: {
+          STV(z, LDV(zs));
+          const int sstat = st.sstat;
           st.p_status = sstat;
-          st.p_t = seg_t(st, s).re;
-          st.p_nacc = sacc;
-          st.p_nrej = srej;
+          st.p_t = seg_t(st, st.s).re;
+          st.p_nacc = st.sacc;
+          st.p_nrej = st.srej;
           if (sstat != PHC_PATH_SUCCESS)
             pc = PC_FINISH;
           else if (!O.so.use_endgame)
@@ -508,12 +567,13 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           else
             pc = PC_EG_INIT;
           break;
+        }
 
         // ---------------- cauchy_endgame, src/endgame.f90:124-267 --------------
         case PC_EG_INIT:
           st.eg_segstep = 1.0;  // segopts: step_init = step_max = 1, grow_after = 2
           st.eg_status = PHC_ENDGAME_FAILED;
-          STV(resz, z);
+          STV(resz, LDV(z));
           st.r = EO.t_start;
           st.have_prev = 0;
           st.best_resid = kHuge;
@@ -571,8 +631,9 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
             pc = PC_EG_DONE;
             break;
           }
+          const cd z = LDV(z);
           STV(zold, z);
-          zs = z;
+          STV(zs, z);
           st.seg_arc = 0;
           st.seg_t0[0] = st.r;
           st.seg_t0[1] = 0.0;
@@ -587,13 +648,13 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
         }
 
         case PC_EG_AFTER_RADIAL: {
-          z = zs;
-          st.eg_segstep = fmin(fmax(step, TO.step_min), 1.0);
-          st.eg_nacc += sacc;
-          st.eg_nrej += srej;
+          cd z = LDV(zs);
+          st.eg_segstep = fmin(fmax(st.step, TO.step_min), 1.0);
+          st.eg_nacc += st.sacc;
+          st.eg_nrej += st.srej;
           const cd zold = LDV(zold);
-          if (sstat != PHC_PATH_SUCCESS) {
-            z = zold;
+          if (st.sstat != PHC_PATH_SUCCESS) {
+            STV(z, zold);
             if (!(st.gate || st.r < EO.loop_radius)) {
               st.lp_max = EO.max_winding;
               st.lp_cont = PC_EG_AFTER_FALLBACK;
@@ -603,6 +664,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
             }
             break;
           }
+          STV(z, z);
           st.r = st.rnew;
           // winding number estimate from the radial differences
           const double d = vnorm(z - zold, lane, N);
@@ -635,10 +697,11 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           }
           break;
 
-        case PC_LOOPS_BEGIN:
+        case PC_LOOPS_BEGIN: {
+          const cd z = LDV(z);
           st.lp_dth = 2.0 * kPi / (double)EO.nsamples;
           st.lp_floor = 10.0 * TO.corrector_tol * vnorm(z, lane, N);
-          zs = z;
+          STV(zs, z);
           STV(zsum, czero<double>());
           st.lp_nsamp = 0;
           st.lp_spacing = kHuge;
@@ -646,8 +709,10 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           st.lp_j = 1;
           pc = PC_LOOP_ARC;
           break;
+        }
 
-        case PC_LOOP_ARC:
+        case PC_LOOP_ARC: {
+          const cd zs = LDV(zs);
           STV(zsum, LDV(zsum) + zs);
           ++st.lp_nsamp;
           STV(zprev, zs);
@@ -661,16 +726,18 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           st.seg_cont = PC_LOOP_AFTER_ARC;
           pc = PC_SEG_BEGIN;
           break;
+        }
 
         case PC_LOOP_AFTER_ARC: {
-          st.eg_segstep = fmin(fmax(step, TO.step_min), 1.0);
-          st.eg_nacc += sacc;
-          st.eg_nrej += srej;
-          if (sstat != PHC_PATH_SUCCESS) {
+          st.eg_segstep = fmin(fmax(st.step, TO.step_min), 1.0);
+          st.eg_nacc += st.sacc;
+          st.eg_nrej += st.srej;
+          if (st.sstat != PHC_PATH_SUCCESS) {
             st.lp_ok = 0;
             pc = st.lp_cont;
             break;
           }
+          const cd zs = LDV(zs);
           st.lp_spacing = fmin(st.lp_spacing, vnorm(zs - LDV(zprev), lane, N));
           const int j = st.lp_j + 1;
           st.lp_j = j;
@@ -678,7 +745,8 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
             pc = PC_LOOP_ARC;
             break;
           }
-          if (vnorm(zs - z, lane, N) <= fmax(EO.closure_factor * st.lp_spacing, st.lp_floor)) {
+          if (vnorm(zs - LDV(z), lane, N) <=
+              fmax(EO.closure_factor * st.lp_spacing, st.lp_floor)) {
             const double inv = (double)st.lp_nsamp;
             const cd zsum = LDV(zsum);
             STV(est, mkc<double>(zsum.re / inv, zsum.im / inv));
@@ -705,12 +773,12 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           if (st.have_prev)
             err = vnorm(est - LDV(prev), lane, N) / fmax(vnorm(est, lane, N), kTiny);
           st.rec_err = err;
-          uk = UK_BACKERR;
-          u_prec = 0;
-          zin = est;
-          tin = czero<double>();
-          dtin = czero<double>();
-          pc_after = PC_RECORD_AFTER;
+          st.uk = UK_BACKERR;
+          st.u_prec = 0;
+          STV(zin, est);
+          st.tin[0] = st.tin[1] = 0.0;
+          st.dtin[0] = st.dtin[1] = 0.0;
+          st.pc_after = PC_RECORD_AFTER;
           want = true;
           break;
         }
@@ -718,6 +786,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
         case PC_RECORD_AFTER: {
           ++st.c_eval;
           const double err = st.rec_err;
+          const cd zin = LDV(zin);
           const double resid = U.a1 / fmax(U.a2 * vnorm(zin, lane, N), kTiny);
           if (st.eg_status == PHC_ENDGAME_FAILED ||
               better(resid, err, st.best_resid, st.eg_error, EO.residual_tol)) {
@@ -741,7 +810,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
             st.p_status = PHC_PATH_ENDGAME_FAILED;
             pc = PC_FINISH;
           } else {
-            z = LDV(resz);
+            STV(z, LDV(resz));
             st.p_t = 0.0;
             st.p_wind = st.eg_wind;
             st.p_egs = st.eg_status;
@@ -752,14 +821,14 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
 
         // ---------------- classify, src/solve.f90:288-328 ---------------------
         case PC_CL_START:
-          uk = UK_COND;
-          u_prec = 0;
-          zin = z;
-          tin = czero<double>();
-          dtin = czero<double>();
+          st.uk = UK_COND;
+          st.u_prec = 0;
+          STV(zin, LDV(z));
+          st.tin[0] = st.tin[1] = 0.0;
+          st.dtin[0] = st.dtin[1] = 0.0;
           st.cond_c0 = 0;
           st.cond_ret = PC_CL_AFTER_COND1;
-          pc_after = PC_COND_STEP;
+          st.pc_after = PC_COND_STEP;
           want = true;
           break;
 
@@ -777,8 +846,8 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           st.cond_ainv = ainv;
           if (c0 + kCondChunk < N) {
             st.cond_c0 = c0 + kCondChunk;
-            uk = UK_COND;
-            pc_after = PC_COND_STEP;
+            st.uk = UK_COND;
+            st.pc_after = PC_COND_STEP;
             want = true;
             break;
           }
@@ -798,10 +867,10 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           if (!sing && O.so.refine_maxit >= 1) {
             // refine, src/solve.f90:254-286
             st.rf_it = 1;
-            dnorm_prev = kHuge;
-            uk = UK_REFINE;
-            zin = z;
-            pc_after = PC_CL_AFTER_REFINE;
+            st.dnorm_prev = kHuge;
+            st.uk = UK_REFINE;
+            STV(zin, LDV(z));
+            st.pc_after = PC_CL_AFTER_REFINE;
             want = true;
           } else {
             pc = sing ? PC_CL_FINAL : PC_CL_COND2;
@@ -816,36 +885,37 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
             break;
           }
           const double dnorm = vnorm(U.x, lane, N);
-          if (dnorm > dnorm_prev) {
+          if (dnorm > st.dnorm_prev) {
             pc = PC_CL_COND2;
             break;
           }
-          z = z + U.x;
+          const cd z = LDV(z) + U.x;
+          STV(z, z);
           if (dnorm <= 4.0 * kEps * vnorm(z, lane, N)) {
             pc = PC_CL_COND2;
             break;
           }
-          dnorm_prev = dnorm;
+          st.dnorm_prev = dnorm;
           const int it = st.rf_it + 1;
           st.rf_it = it;
           if (it > O.so.refine_maxit) {
             pc = PC_CL_COND2;
             break;
           }
-          uk = UK_REFINE;
-          zin = z;
-          pc_after = PC_CL_AFTER_REFINE;
+          st.uk = UK_REFINE;
+          STV(zin, z);
+          st.pc_after = PC_CL_AFTER_REFINE;
           want = true;
           break;
         }
 
         case PC_CL_COND2:
-          uk = UK_COND;
-          u_prec = 0;
-          zin = z;
+          st.uk = UK_COND;
+          st.u_prec = 0;
+          STV(zin, LDV(z));
           st.cond_c0 = 0;
           st.cond_ret = PC_CL_AFTER_COND2;
-          pc_after = PC_COND_STEP;
+          st.pc_after = PC_COND_STEP;
           want = true;
           break;
 
@@ -858,6 +928,7 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
           break;
 
         case PC_CL_FINAL: {
+          const cd z = LDV(z);
           const double znorm = vnorm(z, lane, N);
           const double ri =
               (lane < n) ? cabs(LDV(hsave)) / rpowi(znorm, P.deg[lane]) : 0.0;
@@ -902,16 +973,19 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
             o.endgame_error = st.p_ege;
             o.cond = st.p_cond;
             o.residual = st.p_resid;
-            *rec = o;
+            *st.rec = o;
           }
+          double* zo_ = st.zo;
+          double* xo_ = st.xo;
           if (lane < N) {
-            zo[2 * lane] = z.re;
-            zo[2 * lane + 1] = z.im;
+            const cd z = LDV(z);
+            zo_[2 * lane] = z.re;
+            zo_[2 * lane + 1] = z.im;
           }
-          if (xo != nullptr && lane < n) {
+          if (xo_ != nullptr && lane < n) {
             const cd xv = LDV(xv);
-            xo[2 * lane] = xv.re;
-            xo[2 * lane + 1] = xv.im;
+            xo_[2 * lane] = xv.re;
+            xo_[2 * lane + 1] = xv.im;
           }
           __syncwarp();
           return;
@@ -919,11 +993,18 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
       }
     }
     // ---- run the requested unit ----
-    run_unit<NM, kMixed, EVAL32, F>(C, ws, uk, kMixed ? u_prec : 0, st.cond_c0, zin, tin, dtin, lane,
-                            U);
-    if (kMixed && u_prec == 0 && uk <= UK_NEWTON) ++st.c_retry;  // predictor/corrector unit in FP64
-    ++st.units;
-    pc = pc_after;
+    {
+      const int uk = st.uk;
+      const int u_prec = kMixed ? st.u_prec : 0;
+      const cd zin = LDV(zin);
+      const cd tin = mkc<double>(st.tin[0], st.tin[1]);
+      const cd dtin = mkc<double>(st.dtin[0], st.dtin[1]);
+      run_unit<NM, kMixed, EVAL32, F>(tbl, wbase, uk, u_prec, st.cond_c0, zin, tin, dtin, lane,
+                                      U);
+      if (kMixed && u_prec == 0 && uk <= UK_NEWTON) ++st.c_retry;  // predictor/corrector unit in FP64
+      ++st.units;
+    }
+    pc = st.pc_after;
   }
 }
 
@@ -931,41 +1012,33 @@ __device__ __forceinline__ void track_one(const PlanHeader& P, const WarpConst& 
 #undef LDV
 #undef STV
 
-// Workspace pointers of a warp inside its shared-memory region.
-template <int PREC>
-__device__ __forceinline__ WarpWS warp_workspace(const PlanHeader& P, unsigned char* wbase,
-                                                WarpState** st) {
-  const WsLayout L = ws_layout(P.n, P.S, P.pw_total, PREC == PHC_PREC_MIXED);
-  WarpWS ws;
-  ws.pwd = reinterpret_cast<cd*>(wbase + L.pwd);
-  ws.pwf = reinterpret_cast<cf*>(wbase + L.pwf);
-  ws.jd = reinterpret_cast<cd*>(wbase + L.jd);
-  ws.jf = reinterpret_cast<cf*>(wbase + L.jf);
-  ws.piv = reinterpret_cast<int*>(wbase + L.piv);
-  *st = reinterpret_cast<WarpState*>(wbase + L.st);
-  return ws;
-}
-
 // Structural zeros of the Jacobian are never written by the schedule, so
 // the buffer is cleared once per system; row n holds the patch a (the last
 // row of H_z).
-template <int PREC>
-__device__ __forceinline__ void init_jacobian_buffer(const PlanHeader& P, const WarpWS& ws,
+template <bool EVAL32>
+__device__ __forceinline__ void init_jacobian_buffer(const PlanHeader& P, unsigned char* wbase,
                                                      int lane) {
+  const WarpWS ws = warp_workspace<EVAL32>(P, wbase);
   for (int q = lane; q < (P.n + 1) * P.S; q += kWarp) {
     const int row = q / P.S, col = q - row * P.S;
     cd v = czero<double>();
     if (row == P.n && col < P.N) v = mkc<double>(P.patch[col][0], P.patch[col][1]);
     sts(&ws.jd[q], v);
-    if (PREC == PHC_PREC_MIXED) sts(&ws.jf[q], ccast<float>(v));
+    if (EVAL32) sts(&ws.jf[q], ccast<float>(v));
   }
   __syncwarp();
 }
 
+// Threads per block the kernels of a row width are compiled for.
+template <int NM>
+constexpr int kMaxBlockThreads = max_warps_per_block(NM) * kWarp;
+
 // Single-system kernel: every block stages the table once for its warps.
 template <int NM, int PREC, int F>
-__global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
+__global__ void __launch_bounds__(kMaxBlockThreads<NM>) track_kernel(const KParams kp) {
   extern __shared__ __align__(16) unsigned char smem[];
+  // the single-system kernels of narrow rows carry the FP32 evaluation
+  constexpr bool E32 = kernel_eval32(NM, PREC);
   const int tid = threadIdx.x;
   {
     const int4* src = reinterpret_cast<const int4*>(kp.plan);
@@ -976,11 +1049,9 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
   __syncthreads();
   const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(smem);
   const int warp = tid >> 5, lane = tid & 31;
-  WarpState* stp;
-  const WarpWS ws = warp_workspace<PREC>(P, smem + kp.plan_bytes + warp * kp.ws_bytes, &stp);
-  const WarpConst C = load_warp_const(P, smem, lane);
-  init_jacobian_buffer<PREC>(P, ws, lane);
-  const int n = P.n, N = P.N;
+  unsigned char* wbase = smem + kp.plan_bytes + warp * kp.ws_bytes;
+  WarpState* stp = warp_state<E32>(P, wbase);
+  init_jacobian_buffer<E32>(P, wbase, lane);
   // one call site of the path state machine: a persistent warp pulls paths
   // from the atomic queue, a grid warp takes exactly one
   long long q = -1, qend = 0;
@@ -1000,9 +1071,9 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
       qend = q + 1;
       if (q >= kp.count) break;
     }
-    track_one<NM, PREC, PREC == PHC_PREC_MIXED && NM <= 8, F>(P, C, ws, *stp, kp.opts, kp.k0 + q,
-                                                             lane, kp.out + q,
-                        kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
+    const int n = P.n, N = P.N;
+    track_one<NM, PREC, E32, F>(smem, wbase, *stp, kp.opts, kp.k0 + q, lane, kp.out + q,
+                                kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
   }
 }
 
@@ -1011,7 +1082,8 @@ __global__ void __launch_bounds__(256) track_kernel(const KParams kp) {
 // one queue; a warp that moves on to another system stages that system's
 // table and options into its own shared-memory slice.
 template <int NM, int PREC, int F>
-__global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb) {
+__global__ void __launch_bounds__(kMaxBlockThreads<NM>)
+    track_batch_kernel(const KParamsBatch kb) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char* slice = smem + warp * kb.slice_bytes;
@@ -1052,21 +1124,16 @@ __global__ void __launch_bounds__(256) track_batch_kernel(const KParamsBatch kb)
       unsigned long long* odst = reinterpret_cast<unsigned long long*>(opts);
       for (int v = lane; v < (int)(sizeof(KOpts) >> 3); v += kWarp) odst[v] = osrc[v];
       __syncwarp();
-      WarpState* stp;
-      const WarpWS ws0 = warp_workspace<PREC>(*reinterpret_cast<const PlanHeader*>(tbl), wbase,
-                                              &stp);
-      init_jacobian_buffer<PREC>(*reinterpret_cast<const PlanHeader*>(tbl), ws0, lane);
+      init_jacobian_buffer<false>(*reinterpret_cast<const PlanHeader*>(tbl), wbase, lane);
     }
     const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(tbl);
-    WarpState* stp;
-    const WarpWS ws = warp_workspace<PREC>(P, wbase, &stp);
-    const WarpConst C = load_warp_const(P, tbl, lane);
+    WarpState* stp = warp_state<false>(P, wbase);
     const long long kl = q - S.path_begin;  // 0-based path of the request
     const int n = P.n, N = P.N;
     phc_path_out* out = reinterpret_cast<phc_path_out*>(kb.base + S.out_off) + kl;
     double* z = reinterpret_cast<double*>(kb.base + S.z_off) + 2 * kl * N;
     double* x = S.x_off >= 0 ? reinterpret_cast<double*>(kb.base + S.x_off) + 2 * kl * n : nullptr;
-    track_one<NM, PREC, false, F>(P, C, ws, *stp, *opts, kl + 1, lane, out, z, x);
+    track_one<NM, PREC, false, F>(tbl, wbase, *stp, *opts, kl + 1, lane, out, z, x);
     if (kb.done != nullptr) {
       // every lane's result stores are made visible system-wide before the
       // path is counted as finished
