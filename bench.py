@@ -1,26 +1,32 @@
-"""Benchmark of the B200 path tracker on the batched-paths configuration:
-n = 10 variables, all degrees 2, 20 distinct monomials (of 66) per
-equation with complex normal coefficients, 1024 total-degree paths.
+"""Benchmark of the B200 path tracker on the large single system:
+n = 16 variables, all degrees 2, 24 distinct monomials (of 153) per
+equation with complex normal coefficients, 65,536 total-degree paths.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A step is one pass of the tracker over all 1024 paths of the system
+A step is one pass of the tracker over all 65,536 paths of the system
 (start_solution + track + Cauchy end game + classify numerics), i.e. the
 per-path work of one solve(). Metric: paths/s (higher is better).
 
   value   mixed-precision persistent tracker, inputs (the compiled sparse
           table) resident in device memory, timed with CUDA events on the
           launching stream, L2 flushed (256 MiB written) between timed steps
-  e2e     the same metric through the public C ABI phc_solve_sparse (host
-          table in, host results out through page-locked buffers, host
-          bookkeeping included), wall clock per call
-  fp64    the plain all-FP64 tracker, one warp per path, no refill, same
-          timing as value (the baseline of the mixed-precision target)
+  e2e     the same metric through the public C ABI: phc_solve_sparse on one
+          GPU (host table in, host results out through page-locked buffers,
+          host bookkeeping included), wall clock per call; on N GPUs each
+          rank calls phc_solve_paths on its path range with host buffers,
+          the records are gathered to rank 0 and phc_finish_solve runs the
+          bookkeeping there
+  fp64    the plain all-FP64 tracker, same schedule and timing as value (the
+          baseline of the mixed-precision target)
 
-Under torchrun each rank solves its own system instance of the same shape
-(weak scaling, no collective on the data path); times are the max over
-ranks. --impl reference times the reference's CPU algorithm (the C++
-restatement under oracle/, all host threads) on the same workload.
+Under torchrun the system's paths are split into contiguous ranges, one per
+rank (src/solve.f90:190-208: paths are independent), so the total work is
+fixed (strong scaling); times are the max over ranks, and no collective
+touches the data path. The key `replicas` times one whole system per rank
+(weak scaling) beside it. --impl reference times the reference's CPU
+algorithm (the C++ restatement under oracle/, all host threads) on the same
+system, a bounded sample of its paths per step.
 """
 import argparse
 import ctypes
@@ -39,8 +45,13 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 METRIC = "paths/s mixed vs FP64 at <=1e-10 endpoint err"
-WORKLOAD = ("batched paths: n=10, degrees 2, 20 of 66 monomials per equation, complex "
-            "normal coefficients, 1024 total-degree paths, end game on")
+WORKLOAD = ("large single system: n=16, degrees 2, 24 of 153 monomials per equation, complex "
+            "normal coefficients, 65536 total-degree paths, end game on")
+WORKLOAD_N10 = ("batched paths: n=10, degrees 2, 20 of 66 monomials per equation, complex "
+                "normal coefficients, 1024 total-degree paths, end game on")
+# paths of the restatement per step of the reference arm (a bounded sample
+# of the 65,536: a window of consecutive paths, a different one each step)
+REF_SAMPLE_PATHS = 1024
 
 
 def parse():
@@ -51,18 +62,23 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-n10", action="store_true",
+                    help="skip the secondary n=10, 1024-path measurement")
     ap.add_argument("--serving-systems", type=int, default=4096,
                     help="systems in the serving stream (0 skips the serving leg)")
+    ap.add_argument("--replica-steps", type=int, default=3,
+                    help="N > 1: timed steps of the replicas key (one whole system per "
+                         "rank); 0 skips it")
+    ap.add_argument("--max-paths", type=int, default=0,
+                    help="track only the first N paths of the system (a small case for "
+                         "profiler captures; the line says so)")
     ap.add_argument("--configs", action="store_true",
                     help="instead of the benchmark line, measure the other single-system "
-                         "configurations (n=4 dense quadratic; n=4 singular cubic; n=16 with "
-                         "65536 paths): one JSON line each")
+                         "configurations (n=4 dense quadratic; n=4 singular cubic; n=10 with "
+                         "1024 paths; n=16 with 65536 paths): one JSON line each")
     ap.add_argument("--config-filter", default="",
                     help="with --configs: only the configurations whose description "
                          "contains this text")
-    ap.add_argument("--max-paths", type=int, default=0,
-                    help="with --configs: track only the first N paths of each system "
-                         "(a small case for profiler captures; the line says so)")
     ap.add_argument("--no-tune", action="store_true",
                     help="default launch configuration instead of the autotuner's "
                          "(for profiling: the timed launches then follow the warm-up directly)")
@@ -74,31 +90,46 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
-def workload(rank=0):
+def workload():
     from polyhomocont_b200 import workloads as W
-    return W.cfg2(seed=W.seed_for(2, rank))
+    return W.cfg5()
+
+
+def sample_windows(npaths, count, nwin):
+    """nwin windows of `count` consecutive 1-based paths, spread evenly over
+    1..npaths (the first starts at path 1, the last ends at npaths)."""
+    if nwin <= 1:
+        return [1]
+    span = npaths - count
+    return [1 + (span * w) // (nwin - 1) for w in range(nwin)]
 
 
 # ---------------------------------------------------------------------------
 # CPU baseline: the C++ restatement of the reference (oracle/), all threads
 # ---------------------------------------------------------------------------
-def cpu_paths_per_s(min_seconds=3.0, max_reps=50):
+def cpu_paths_per_s(min_seconds=10.0, max_windows=16):
+    """The restatement on all host threads over windows of the system's
+    paths (REF_SAMPLE_PATHS each, spread over the range) until about
+    min_seconds have passed."""
     from oracle import oracle as O
     from polyhomocont_b200 import workloads as W
     O.build()
-    n, eqs = workload(0)
+    n, eqs = workload()
     s = W.build(lambda: O.SparseSystem(fast=True), n, eqs)
     threads = os.cpu_count() or 1
-    L = O.lib(fast=True)
-    npaths = int(L.orc_bezout(s.h))
-    reps, t0 = 0, time.perf_counter()
-    while True:
-        O.solve_paths(s, nthreads=threads)
-        reps += 1
+    npaths = int(O.lib(fast=True).orc_bezout(s.h))
+    wins = sample_windows(npaths, REF_SAMPLE_PATHS, max_windows)
+    done, t0 = 0, time.perf_counter()
+    for k0 in wins:
+        O.solve_paths(s, k0=k0, count=REF_SAMPLE_PATHS, nthreads=threads)
+        done += 1
         el = time.perf_counter() - t0
-        if el >= min_seconds or reps >= max_reps:
+        if el >= min_seconds:
             break
-    return npaths * reps / el, threads, f"all {npaths} paths x {reps} solves, {threads} threads", el
+    paths = done * REF_SAMPLE_PATHS
+    return (paths / el, threads,
+            f"{paths} of the {npaths} paths ({done} windows of {REF_SAMPLE_PATHS} consecutive "
+            f"paths spread over the range), {threads} threads", el)
 
 
 def cpu_serving_baseline(nsys_max=512, max_seconds=10.0):
@@ -131,32 +162,41 @@ def cpu_serving_baseline(nsys_max=512, max_seconds=10.0):
 
 
 def run_reference(args):
+    """The reference's algorithm on the host cores (the C++ restatement,
+    -O3, all threads; no Fortran compiler exists for the reference itself)
+    on the same system: each step tracks a window of REF_SAMPLE_PATHS
+    consecutive paths, the windows spread over the 65,536 paths."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     from oracle import oracle as O
     from polyhomocont_b200 import workloads as W
     O.build()
-    n, eqs = workload(0)
+    n, eqs = workload()
     s = W.build(lambda: O.SparseSystem(fast=True), n, eqs)
     threads = os.cpu_count() or 1
     npaths = int(O.lib(fast=True).orc_bezout(s.h))
-    for _ in range(max(args.warmup, 0)):
-        O.solve_paths(s, nthreads=threads)
+    steps = max(args.steps, 1)
+    wins = sample_windows(npaths, REF_SAMPLE_PATHS, max(args.warmup, 0) + steps)
+    for k0 in wins[:max(args.warmup, 0)]:
+        O.solve_paths(s, k0=k0, count=REF_SAMPLE_PATHS, nthreads=threads)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        O.solve_paths(s, nthreads=threads)
+    for k0 in wins[max(args.warmup, 0):]:
+        O.solve_paths(s, k0=k0, count=REF_SAMPLE_PATHS, nthreads=threads)
     el = time.perf_counter() - t0
-    v = npaths * args.steps / el
+    v = REF_SAMPLE_PATHS * steps / el
+    sample = (f"{REF_SAMPLE_PATHS} consecutive paths per step, windows spread over the "
+              f"{npaths} paths, {threads} threads (C++ restatement of the reference, -O3; "
+              "no Fortran compiler for the reference itself)")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "paths/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "paths": npaths, "threads": threads},
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "paths": npaths,
+                   "paths_per_step": REF_SAMPLE_PATHS, "threads": threads},
         "cpu_baseline": {"value": v, "unit": "paths/s", "cores": threads, "kind": "port",
-                         "sample": f"all {npaths} paths per step, {threads} threads "
-                                   "(C++ restatement; no Fortran compiler for the reference)"},
+                         "sample": sample},
         "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -222,12 +262,15 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # serving: stream of random sparse systems (n ~ U{2..8}, d_i ~ U{2,3})
 # ---------------------------------------------------------------------------
-# DRAM bytes (read + write) of one mixed-precision launch on this workload,
-# from `ncu --set full --clock-control none -k regex:track_kernel -c 2` of
-# `python bench.py --steps 2 --warmup 3 --no-e2e --no-cpu --serving-systems 0`
-# (profiles/track_kernel_n10_1024paths.md). The kernel is compute- and
-# latency-bound; its traffic is the table, the start data and the results.
-NCU_DRAM_BYTES_PER_LAUNCH = 123904
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
+# mixed-precision launch of the tracker on the first 4,736 paths of this
+# system, from
+#   ncu --set full --clock-control none -k regex:track_kernel -s 3 -c 1
+#   python bench.py --configs --config-filter large --max-paths 4736 --no-tune
+#       --steps 1 --warmup 3
+# The kernel is compute- and latency-bound: its DRAM traffic is the table,
+# the kernel's code and the path records, most of which stay in L2.
+NCU_DRAM_BYTES = {"bytes": 521728, "paths": 4736}
 SCHED_NAMES = {0: "grid", 1: "persistent"}
 
 
@@ -306,6 +349,7 @@ def run_configs(args):
          W.dense_quadratic(), None),
         ("singular endpoints: n=4, degrees 3, (x_j - r_j)^2 and ^3 terms, 81 paths, "
          "16 ending at the known root r", (n3, eqs3), r3),
+        (WORKLOAD_N10, W.cfg2(), None),
         ("large single system: n=16, degrees 2, 24 of 153 monomials per equation, "
          "65536 paths", W.cfg5(), None),
     ]
@@ -383,6 +427,67 @@ def run_configs(args):
         print(json.dumps(line), flush=True)
 
 
+def time_launches(stream, flush, launch, k):
+    """Total device time (s) of k launches, each timed with CUDA events on
+    the launching stream after an L2 flush (256 MiB written)."""
+    import torch
+    total = 0.0
+    for _ in range(k):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        launch()
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b) * 1e-3
+    return total
+
+
+def endpoint_agreement(n, pm, zm, pd, zd):
+    """(max relative error of the regular finite endpoints of two runs,
+    whether their classification is identical)."""
+    fin = (pd["status"] == 0) & (pd["at_infinity"] == 0)
+    err = 0.0
+    if fin.any():
+        xm = zm[fin, :n] / zm[fin, n:n + 1]
+        xd = zd[fin, :n] / zd[fin, n:n + 1]
+        err = float(np.max(np.max(np.abs(xm - xd), axis=1) /
+                           np.maximum(1.0, np.max(np.abs(xd), axis=1))))
+    same = all(np.array_equal(pm[k], pd[k]) for k in
+               ("status", "winding_number", "at_infinity", "singular", "is_real"))
+    return err, same
+
+
+def measure_n10(P, W, dev, stream, flush, steps, warmup, local):
+    """The n=10, 1024-path system on one GPU: device-timed paths/s of both
+    precisions, each autotuned (a secondary key of the line)."""
+    import torch
+    n, eqs = W.cfg2()
+    s = W.build(P.SparseSystem, n, eqs)
+    npaths = s.bezout()
+    out = {}
+    for prec, key in ((P.PHC_PREC_MIXED, "mixed"), (P.PHC_PREC_FP64, "fp64")):
+        g, _ = P.autotune(s, gpu=P.default_gpu_options(prec, device=local))
+        plan = P.Plan(s, gpu=g)
+        o = torch.zeros(npaths * 96, dtype=torch.uint8, device=dev)
+        z = torch.zeros(npaths * (n + 1) * 2, dtype=torch.float64, device=dev)
+
+        def launch():
+            plan.launch(1, npaths, o.data_ptr(), z.data_ptr(), stream.cuda_stream)
+        for _ in range(max(warmup, 3)):
+            launch()
+        torch.cuda.synchronize()
+        t = time_launches(stream, flush, launch, steps)
+        out[key] = {"value": npaths * steps / t, "unit": "paths/s",
+                    "ms_per_step": 1e3 * t / steps, "schedule": SCHED_NAMES[g.schedule],
+                    "warps_per_block": plan.config()["warps_per_block"]}
+        plan.close()
+    out["mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["workload"] = WORKLOAD_N10
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -394,7 +499,7 @@ def main():
     rank, world, local = dist_env()
     import torch
     import polyhomocont_b200 as P
-    from polyhomocont_b200 import _abi, flops
+    from polyhomocont_b200 import _abi, flops, shard
     from polyhomocont_b200 import workloads as W
     from polyhomocont_b200 import build as B
 
@@ -413,12 +518,18 @@ def main():
         if pg is not None:
             pg.barrier()
 
-    def max_over_ranks(x):
+    def reduce_over_ranks(x, op):
         if pg is None:
             return x
         t = torch.tensor([x], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        pg.all_reduce(t, op=op)
         return float(t.item())
+
+    def max_over_ranks(x):
+        return reduce_over_ranks(x, pg.ReduceOp.MAX if pg else None)
+
+    def sum_over_ranks(x):
+        return reduce_over_ranks(x, pg.ReduceOp.SUM if pg else None)
 
     L = _abi.lib()
     p64, p32 = ctypes.c_double(), ctypes.c_double()
@@ -427,16 +538,19 @@ def main():
         raise RuntimeError(f"phc_measure_fma_peaks: {_abi.last_error()}")
     peak64, peak32 = p64.value, p32.value
 
-    n, eqs = workload(rank)
+    # one system; this rank's contiguous range of its paths
+    n, eqs = workload()
     sysP = W.build(P.SparseSystem, n, eqs)
-    npaths = sysP.bezout()
+    npaths_sys = sysP.bezout()
+    npaths = min(npaths_sys, args.max_paths) if args.max_paths > 0 else npaths_sys
+    k0, count = shard.path_range(npaths, rank, world)
     t, _ = sysP.table()
     T = sysP.total_terms()
     hexps = np.ctypeslib.as_array(t.hexps, shape=(T * (n + 1),)).reshape(T, n + 1).copy()
     model = flops.unit_model(n, sysP.degrees(), hexps)
 
     # both arms get their launch configuration from the autotuner (timed on
-    # a sample of this system's paths, before and outside the timed region);
+    # a sample of the system's paths, before and outside the timed region);
     # the two arms then differ only in precision and in what the tuner chose
     if args.no_tune:
         g_mixed = P.default_gpu_options(P.PHC_PREC_MIXED, device=local)
@@ -445,79 +559,76 @@ def main():
     else:
         g_mixed, tune_m = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_MIXED,
                                                                      device=local))
-        g_fp64, tune_d = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_FP64,
-                                                                    device=local))
+        g_fp64, _ = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_FP64,
+                                                               device=local))
     plan_m = P.Plan(sysP, gpu=g_mixed)
     plan_d = P.Plan(sysP, gpu=g_fp64)
-    out_m = torch.zeros(npaths * 96, dtype=torch.uint8, device=dev)
-    z_m = torch.zeros(npaths * (n + 1) * 2, dtype=torch.float64, device=dev)
+    out_m = torch.zeros(max(count, 1) * 96, dtype=torch.uint8, device=dev)
+    z_m = torch.zeros(max(count, 1) * (n + 1) * 2, dtype=torch.float64, device=dev)
     out_d = torch.zeros_like(out_m)
     z_d = torch.zeros_like(z_m)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
 
-    def step(plan, out, z):
-        plan.launch(1, npaths, out.data_ptr(), z.data_ptr(), sptr)
+    def launch_m():
+        plan_m.launch(k0, count, out_m.data_ptr(), z_m.data_ptr(), sptr)
 
-    def timed(plan, out, z, k):
-        total = 0.0
-        for _ in range(k):
-            flush.zero_()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            step(plan, out, z)
-            b.record(stream)
-            b.synchronize()
-            total += a.elapsed_time(b) * 1e-3
-        return total
+    def launch_d():
+        plan_d.launch(k0, count, out_d.data_ptr(), z_d.data_ptr(), sptr)
 
     for _ in range(max(args.warmup, 3)):
-        step(plan_m, out_m, z_m)
-        step(plan_d, out_d, z_d)
+        launch_m()
+        launch_d()
     torch.cuda.synchronize()
 
     sampler = ClockSampler(local)
     sampler.start()
     barrier()
     torch.cuda.synchronize()
-    t_mixed = timed(plan_m, out_m, z_m, args.steps)
+    t_mixed = time_launches(stream, flush, launch_m, args.steps)
     torch.cuda.synchronize()
     barrier()
-    t_fp64 = timed(plan_d, out_d, z_d, args.steps)
+    t_fp64 = time_launches(stream, flush, launch_d, args.steps)
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
     t_mixed_max = max_over_ranks(t_mixed)
     t_fp64_max = max_over_ranks(t_fp64)
 
-    value = npaths * world * args.steps / t_mixed_max
-    v_fp64 = npaths * world * args.steps / t_fp64_max
+    value = npaths * args.steps / t_mixed_max
+    v_fp64 = npaths * args.steps / t_fp64_max
 
     # results of the last runs: counters for the flop model, endpoints
-    pm = np.frombuffer(out_m.cpu().numpy().tobytes(), dtype=P.PATH_DTYPE)
-    pd = np.frombuffer(out_d.cpu().numpy().tobytes(), dtype=P.PATH_DTYPE)
-    zm = z_m.cpu().numpy().view(np.complex128).reshape(npaths, n + 1)
-    zd = z_d.cpu().numpy().view(np.complex128).reshape(npaths, n + 1)
-    fin = (pd["status"] == 0) & (pd["at_infinity"] == 0)
-    err = 0.0
-    if fin.any():
-        xm = zm[fin, :n] / zm[fin, n:n + 1]
-        xd = zd[fin, :n] / zd[fin, n:n + 1]
-        err = float(np.max(np.max(np.abs(xm - xd), axis=1) /
-                           np.maximum(1.0, np.max(np.abs(xd), axis=1))))
-    same_class = all(np.array_equal(pm[k], pd[k]) for k in
-                     ("status", "winding_number", "at_infinity", "singular", "is_real"))
+    pm = np.frombuffer(out_m.cpu().numpy().tobytes(), dtype=P.PATH_DTYPE)[:count]
+    pd = np.frombuffer(out_d.cpu().numpy().tobytes(), dtype=P.PATH_DTYPE)[:count]
+    zm = z_m.cpu().numpy().view(np.complex128).reshape(-1, n + 1)[:count]
+    zd = z_d.cpu().numpy().view(np.complex128).reshape(-1, n + 1)[:count]
+    err, same_class = endpoint_agreement(n, pm, zm, pd, zd)
+    err = max_over_ranks(err)
+    same_class = max_over_ranks(0.0 if same_class else 1.0) == 0.0
     f64m, f32m = flops.path_flops(model, pm, mixed=True)
     f64d, _ = flops.path_flops(model, pd, mixed=False)
-    per_launch_s = t_mixed / args.steps
+    per_launch_s = t_mixed / args.steps  # this rank's launch
     achieved = (f64m + f32m) / per_launch_s / 1e12
     t_at_peak = f64m / (peak64 * 1e12) + f32m / (peak32 * 1e12)
     peak_eff = (f64m + f32m) / t_at_peak / 1e12 if t_at_peak > 0 else None
     fp64_achieved = f64d / (t_fp64 / args.steps) / 1e12
+    units = {k: int(sum_over_ranks(float(pm[k].astype(np.int64).sum()))) for k in
+             ("n_tangent", "n_newton", "n_refine", "n_eval", "n_cond", "n_fp64_retry")}
+    units_d = {k: int(sum_over_ranks(float(pd[k].astype(np.int64).sum()))) for k in
+               ("n_tangent", "n_newton", "n_refine", "n_eval", "n_cond")}
+    pred_corr = units["n_tangent"] + units["n_newton"]
+    fp64_share = units["n_fp64_retry"] / pred_corr if pred_corr else None
+    counts = {"regular": int(((pd["status"] == 0) & (pd["at_infinity"] == 0) &
+                              (pd["singular"] == 0)).sum()),
+              "singular": int(((pd["status"] == 0) & (pd["singular"] != 0) &
+                               (pd["at_infinity"] == 0)).sum()),
+              "infinite": int(((pd["status"] == 0) & (pd["at_infinity"] != 0)).sum()),
+              "failed": int((pd["status"] != 0).sum())}
+    counts = {k: int(sum_over_ranks(v)) for k, v in counts.items()}
 
-    # end to end through the public ABI
+    # end to end through the public ABI, host buffers
     e2e = None
     if not args.no_e2e:
         def pinned(shape, dtype):
@@ -528,23 +639,65 @@ def main():
             pinned.keep.append(buf)
             return arr
         pinned.keep = []
-        bufs = P._result_buffers(n, npaths, alloc=pinned)
+        table_bytes = plan_m.config()["table_bytes"]
+        if world == 1 and npaths == npaths_sys:
+            bufs = P._result_buffers(n, npaths, alloc=pinned)
+
+            def e2e_step():
+                res, _ = P.solve(sysP, gpu=g_mixed, buffers=bufs)
+                return res
+            how = ("phc_solve_sparse: host table in, page-locked host results out, host "
+                   "bookkeeping included")
+        else:
+            def runner(kk, cc):
+                p_, z_, x_, st_ = P.solve_paths(sysP, gpu=g_mixed, k0=kk, count=cc)
+                if st_ != 0:
+                    raise RuntimeError(f"solve_paths: status {st_}")
+                return p_, z_, x_
+
+            def e2e_step():
+                return shard.solve_sharded(sysP, rank, world, gpu=g_mixed, runner=runner,
+                                           npaths=npaths)
+            how = ("phc_solve_paths per rank on its path range (host buffers), records "
+                   "gathered to rank 0, phc_finish_solve there")
         for _ in range(2):
-            P.solve(sysP, gpu=g_mixed, buffers=bufs)
+            e2e_step()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            res, st = P.solve(sysP, gpu=g_mixed, buffers=bufs)
+            res = e2e_step()
         t_e2e = time.perf_counter() - t0
         barrier()
         t_e2e = max_over_ranks(t_e2e)
-        cfg = plan_m.config()
-        e2e = {"value": npaths * world * args.steps / t_e2e, "unit": "paths/s",
-               "h2d_bytes_per_step": cfg["table_bytes"],
+        e2e = {"value": npaths * args.steps / t_e2e, "unit": "paths/s",
+               "h2d_bytes_per_step": table_bytes * world,
                "d2h_bytes_per_step": npaths * (96 + 16 * (n + 1) + 16 * n),
-               "ms_per_step": 1e3 * t_e2e / args.steps,
-               "nsolutions": int(res.nsolutions), "ninfinite": int(res.ninfinite),
-               "nfailed": int(res.nfailed)}
+               "ms_per_step": 1e3 * t_e2e / args.steps, "path": how}
+        if rank == 0 and res is not None:
+            e2e.update({"nsolutions": int(res.nsolutions), "ninfinite": int(res.ninfinite),
+                        "nfailed": int(res.nfailed)})
+
+    # one whole system per rank (weak scaling), beside the split above
+    replicas = None
+    if world > 1 and args.replica_steps > 0:
+        out_r = torch.zeros(npaths * 96, dtype=torch.uint8, device=dev)
+        z_r = torch.zeros(npaths * (n + 1) * 2, dtype=torch.float64, device=dev)
+
+        def launch_r():
+            plan_m.launch(1, npaths, out_r.data_ptr(), z_r.data_ptr(), sptr)
+        launch_r()
+        torch.cuda.synchronize()
+        barrier()
+        t_r = max_over_ranks(time_launches(stream, flush, launch_r, args.replica_steps))
+        replicas = {"value": npaths * world * args.replica_steps / t_r, "unit": "paths/s",
+                    "steps": args.replica_steps, "ms_per_step": 1e3 * t_r / args.replica_steps,
+                    "scaling": "weak",
+                    "parallelism": f"{world} replicas (one whole system per GPU)"}
+        del out_r, z_r
+
+    n10 = None
+    if rank == 0 and not args.no_n10:
+        n10 = measure_n10(P, W, dev, stream, flush, args.steps, args.warmup, local)
 
     serve = None
     if args.serving_systems > 0 and rank == 0:
@@ -560,46 +713,57 @@ def main():
 
     if rank == 0:
         cfg = plan_m.config()
+        traffic = NCU_DRAM_BYTES["bytes"] * count / NCU_DRAM_BYTES["paths"]
         line = {
             "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t_mixed_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (complex)",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64 (complex)",
             "data": "synthetic (seeded reference generator)",
-            "config": {"workload": WORKLOAD, "paths": npaths, "precision": "mixed",
+            "config": {"workload": WORKLOAD if npaths == npaths_sys else
+                       f"{WORKLOAD}; first {npaths} paths only",
+                       "paths": npaths, "paths_per_rank": count, "precision": "mixed",
                        "schedule": SCHED_NAMES[g_mixed.schedule],
                        "warps_per_block": cfg["warps_per_block"], "chunk": g_mixed.chunk,
-                       "grid": cfg["grid"],
+                       "grid": cfg["grid"], "row_width": cfg["nm"],
                        "tuned_by": ("defaults (--no-tune)" if args.no_tune else "phc_autotune on "
                                     f"{tune_m['sample_paths']} paths, "
                                     f"{len(tune_m['candidates'])} candidates"),
                        "l2": "flushed between timed steps (256 MiB write)",
-                       "parallelism": f"dp{world} (one system instance per GPU)"},
+                       "parallelism": (f"{world} GPUs, contiguous path ranges of one system"
+                                       if world > 1 else "one GPU")},
             "fp64_plain": {"value": v_fp64, "unit": "paths/s",
                            "schedule": SCHED_NAMES[g_fp64.schedule],
                            "warps_per_block": plan_d.config()["warps_per_block"],
                            "chunk": g_fp64.chunk,
                            "ms_per_step": 1e3 * t_fp64_max / args.steps,
                            "achieved_tflops": fp64_achieved,
-                           "frac_of_fp64_peak": fp64_achieved / peak64},
+                           "frac_of_fp64_peak": fp64_achieved / peak64,
+                           "units": units_d},
             "mixed_vs_fp64": value / v_fp64,
             "endpoint_max_rel_err_mixed_vs_fp64": err,
             "classification_identical_mixed_vs_fp64": bool(same_class),
+            "counts": counts,
+            "units": dict(units, fp64_share_of_predictor_corrector=fp64_share),
             "roofline": {"bound": "fp64+fp32 CUDA-core pipes (no tensor cores, not HBM)",
                          "achieved": achieved, "peak": peak_eff, "unit": "TFLOP/s",
                          "frac": achieved / peak_eff if peak_eff else None,
-                         "traffic": NCU_DRAM_BYTES_PER_LAUNCH,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
-                                           "one --set full capture of this workload "
-                                           "(profiles/track_kernel_n10_1024paths.md)",
+                         "traffic": traffic,
+                         "traffic_source": (
+                             "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                             f"mixed launch on the first {NCU_DRAM_BYTES['paths']} paths of "
+                             f"this system, scaled by paths to this launch's {count}"),
                          "peak_fp64_tflops": peak64, "peak_fp32_tflops": peak32,
-                         "peak_source": "measured live (phc_measure_fma_peaks FMA loop)",
+                         "peak_source": "measured live (phc_measure_fma_peaks FMA loop); "
+                                        "blend weighted by the launch's FP64/FP32 flops",
                          "flops_per_launch": {"fp64": f64m, "fp32": f32m},
                          "f_unit": model["F_unit"]},
             "clocks": clocks,
             "gpu_launches": args.steps,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "replicas": replicas,
+            "n10": n10,
             "serving": serve,
         }
         print(json.dumps(line), flush=True)

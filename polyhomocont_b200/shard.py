@@ -29,20 +29,22 @@ class ShardFailure(RuntimeError):
     reaches the gather (rank 0 names the failed ranks)."""
 
 
-def solve_sharded(sys, rank, world, group=None, options=None, gpu=None, runner=None):
+def solve_sharded(sys, rank, world, group=None, options=None, gpu=None, runner=None,
+                  npaths=None):
     """solve() over `world` ranks. runner(k0, count) -> (paths, z, x) tracks a
     path range; by default the GPU (phc_solve_paths on this rank's device).
-    Returns the SolveResult on rank 0 and None elsewhere.
+    npaths: solve only the first npaths paths (default: all of them).
+    Returns the SolveResult on rank 0 and None elsewhere. With world == 1
+    no process group is needed.
 
     Failure handling: a rank whose tracking raises still takes part in the
     gather, with an error record instead of its paths, so rank 0 learns at
     once which ranks failed and raises ShardFailure, and the failed rank
     re-raises its own error. A rank that dies outright leaves the gather to
     the process group's timeout, which ends it with an error on the others."""
-    import torch.distributed as dist
     from . import default_gpu_options, default_options, solve_paths
     o = options if options is not None else default_options()
-    npaths = sys.bezout()
+    npaths = sys.bezout() if npaths is None else int(npaths)
     n = sys.nvars()
     k0, count = path_range(npaths, rank, world)
     err = None
@@ -58,8 +60,12 @@ def solve_sharded(sys, rank, world, group=None, options=None, gpu=None, runner=N
     except Exception as e:  # reported through the gather, re-raised below
         err = e
         mine = (k0, None, None, f"{type(e).__name__}: {e}")
-    parts = [None] * world if rank == 0 else None
-    dist.gather_object(mine, parts, dst=0, group=group)
+    if world == 1:
+        parts = [mine]
+    else:
+        import torch.distributed as dist
+        parts = [None] * world if rank == 0 else None
+        dist.gather_object(mine, parts, dst=0, group=group)
     if err is not None:
         raise ShardFailure(f"rank {rank} failed to track paths {k0}..{k0 + count - 1}") from err
     if rank != 0:

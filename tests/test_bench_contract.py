@@ -25,7 +25,8 @@ def test_reference_arm_line():
     assert d["impl"] == "reference"
     assert d["unit"] == "paths/s" and d["higher_is_better"] is True
     assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 1
-    assert d["config"]["paths"] == 1024
+    assert d["config"]["paths"] == 65536 and d["config"]["paths_per_step"] >= 1
+    assert d["scaling"] == "strong"
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
     assert d["cpu_baseline"]["kind"] in ("reference", "port")
     assert d["e2e"] == {"value": d["value"], "unit": "paths/s", "h2d_bytes_per_step": 0,
@@ -37,3 +38,12 @@ def test_reference_arm_other_ranks_exit_quietly():
                   "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1")
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_sample_windows_span_the_range():
+    sys.path.insert(0, ROOT)
+    import bench
+    w = bench.sample_windows(65536, 1024, 25)
+    assert w[0] == 1 and w[-1] + 1024 - 1 == 65536
+    assert all(b > a for a, b in zip(w, w[1:]))
+    assert bench.sample_windows(65536, 1024, 1) == [1]

@@ -141,3 +141,26 @@ def test_failed_rank_is_detected(tmp_path, mode):
         assert "ranks failed: 1" in out0 and "injected tracking failure" in out0
         t1, out1 = open(os.path.join(tmp_path, "rank1.txt")).read().split("\n", 1)
         assert out1.startswith("ShardFailure")
+
+
+def test_single_rank_needs_no_process_group(orc):
+    """world == 1 (bench.py on one GPU with a path subset): solve_sharded
+    gathers nothing and finishes the first npaths paths directly."""
+    import polyhomocont_b200 as P
+    from polyhomocont_b200 import shard
+    from polyhomocont_b200 import workloads as W
+    n, eqs = W.cyclic(5)
+    so = W.build(orc.SparseSystem, n, eqs)
+    sp = W.build(P.SparseSystem, n, eqs)
+
+    def runner(k0, count):
+        p, z, x, st = orc.solve_paths(so, k0=k0, count=count)
+        assert st == 0
+        return p, z, x
+
+    res = shard.solve_sharded(sp, 0, 1, runner=runner, npaths=40)
+    p, z, x, st = orc.solve_paths(so, k0=1, count=40)
+    ref = P.result_from_arrays(n, p, x)
+    assert res.npaths == 40
+    assert np.array_equal(res.paths["solution_index"], ref.paths["solution_index"])
+    assert res.nsolutions == ref.nsolutions and res.ninfinite == ref.ninfinite
