@@ -1,5 +1,12 @@
-"""Helpers mirroring the reference's test/testing.f90."""
+"""Helpers mirroring the reference's test/testing.f90, and the parity
+check of a GPU solve() against the restatement's."""
 import numpy as np
+
+# finite regular endpoints: relative max-norm error (the tracker's
+# corrector tolerance is 1e-10); singular endpoints: the reference's
+# singular_dedup_tol, since such endpoints are less accurate
+TOL_REGULAR = 1e-10
+TOL_SINGULAR = 1e-6
 
 
 def set_distance(a, b):
@@ -158,3 +165,28 @@ def reference_bookkeeping(n, paths, x, o):
                 singular_solutions=np.array(ssols, dtype=np.complex128).reshape(len(ssols), n),
                 multiplicities=np.array(mult, dtype=np.int32),
                 real_solutions=np.array(reals).reshape(len(reals), n))
+
+
+def assert_parity(n, ref, got):
+    """Parity of a GPU solve() result with the restatement's: identical
+    counts, multiplicities and per-path status, winding number,
+    classification, solution/singular indices and end game status; finite
+    regular endpoints within TOL_REGULAR (relative, max norm) and the
+    singular solution sets within TOL_SINGULAR."""
+    assert got.npaths == ref.npaths
+    for key in ("nsolutions", "nreal", "nsingular", "ninfinite", "nfailed", "nduplicates"):
+        assert getattr(got, key) == getattr(ref, key), key
+    assert list(got.multiplicities) == list(ref.multiplicities)
+    for key in ("status", "winding_number", "at_infinity", "singular", "is_real",
+                "solution_index", "singular_index", "endgame_status"):
+        assert np.array_equal(got.paths[key], ref.paths[key]), (
+            key, np.nonzero(got.paths[key] != ref.paths[key])[0][:10])
+    reg = (ref.paths["solution_index"] > 0)
+    if reg.any():
+        d = np.max(np.abs(got.x[reg] - ref.x[reg]), axis=1) / np.maximum(
+            1.0, np.max(np.abs(ref.x[reg]), axis=1))
+        assert d.max() <= TOL_REGULAR, d.max()
+        assert set_distance(got.solutions, ref.solutions) <= TOL_REGULAR
+    sing = (ref.paths["singular_index"] > 0)
+    if sing.any():
+        assert set_distance(got.singular_solutions, ref.singular_solutions) <= TOL_SINGULAR

@@ -17,13 +17,11 @@ import pytest
 
 import polyhomocont_b200 as P
 from polyhomocont_b200 import workloads as W
-from tests.helpers import set_distance
+from tests.helpers import TOL_REGULAR, assert_parity, set_distance
 
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-TOL_REGULAR = 1e-10
-TOL_SINGULAR = 1e-6
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -68,26 +66,6 @@ def solve_both(orc, name, precision, options=None, schedule=P.PHC_SCHED_PERSISTE
     got, st2 = P.solve(sp, po, g)
     assert st1 == st2 == 0
     return n, ref, got
-
-
-def assert_parity(n, ref, got):
-    assert got.npaths == ref.npaths
-    for key in ("nsolutions", "nreal", "nsingular", "ninfinite", "nfailed", "nduplicates"):
-        assert getattr(got, key) == getattr(ref, key), key
-    assert list(got.multiplicities) == list(ref.multiplicities)
-    for key in ("status", "winding_number", "at_infinity", "singular", "is_real",
-                "solution_index", "singular_index", "endgame_status"):
-        assert np.array_equal(got.paths[key], ref.paths[key]), (
-            key, np.nonzero(got.paths[key] != ref.paths[key])[0][:10])
-    reg = (ref.paths["solution_index"] > 0)
-    if reg.any():
-        d = np.max(np.abs(got.x[reg] - ref.x[reg]), axis=1) / np.maximum(
-            1.0, np.max(np.abs(ref.x[reg]), axis=1))
-        assert d.max() <= TOL_REGULAR, d.max()
-        assert set_distance(got.solutions, ref.solutions) <= TOL_REGULAR
-    sing = (ref.paths["singular_index"] > 0)
-    if sing.any():
-        assert set_distance(got.singular_solutions, ref.singular_solutions) <= TOL_SINGULAR
 
 
 @pytest.mark.parametrize("precision", [P.PHC_PREC_FP64, P.PHC_PREC_MIXED])
@@ -158,12 +136,12 @@ def test_cfg2_parity_sample(orc):
         assert d.max() <= TOL_REGULAR
 
 
-@pytest.mark.parametrize("n", [16, 20, 28, 31])
+@pytest.mark.parametrize("n", [12, 16, 17, 20, 28, 31])
 def test_wide_rows_parity_sample(orc, n):
-    """Random sparse quadratic systems whose N = n+1 unknowns need the wider
-    register rows (18, 24, 32 columns: the elimination without column-group
-    branches for 24 and 32, spilling kernels included), up to the maximum
-    N = 32; first 24 paths, both precisions, against the restatement."""
+    """Random sparse quadratic systems of every register-row width above the
+    benchmark systems' (12, 16, 18, 24 and 32 columns), up to the maximum
+    N = n + 1 = 32 unknowns; first 24 paths, both precisions, against the
+    restatement."""
     n_, eqs = W.sparse_quadratic(n, 24, W.seed_for(5, 100 + n))
     if n == 31:
         # 2^31 paths exceed the reference's integer bound (src/homotopy.f90:128-132):
