@@ -317,6 +317,8 @@ struct WarpConst {
   const cf* coeff;
   const uint2* meta;
   const double (*patch)[2];
+  int red_c;                   // pivot column of the patch row (see evaluate_reduced)
+  const double (*rho)[2];      // rho_j = a_j / a_c
 };
 
 __device__ __forceinline__ WarpConst load_warp_const(const PlanHeader& P,
@@ -339,6 +341,8 @@ __device__ __forceinline__ WarpConst load_warp_const(const PlanHeader& P,
   C.coeff = reinterpret_cast<const cf*>(pb + P.off_jf);
   C.meta = reinterpret_cast<const uint2*>(pb + P.off_jm);
   C.patch = P.patch;
+  C.red_c = P.red_c;
+  C.rho = P.rho;
   return C;
 }
 
@@ -448,85 +452,22 @@ template <> __device__ __forceinline__ const cf* plan_coef<float>(const unsigned
   return reinterpret_cast<const cf*>(pb + off_f);
 }
 
-// Homotopy H(z,t) = gamma t G(z) + (1 - t) F^h(z) plus the patch row
-// (tdh_evaluate, src/homotopy.f90:188-231), in precision T. Input: lane j
-// holds z_j. Output: lane i holds row i of H_z in a[] (zero beyond N),
-// and h_i, ht_i. F^h_i is obtained from row i of its Jacobian by Euler's
-// relation for homogeneous polynomials, F^h_i = (1/d_i) sum_j z_j dF^h_i/dz_j,
-// which needs no evaluation of its own.
-// F: the schedule form the kernel was compiled for (the most power-table
-// factors of any record: 1, 2 or 3).
-template <int NM, typename T, int F>
-__device__ __forceinline__ void evaluate(const WarpConst& C, const WarpWS& ws, cd zl, cd t,
-                                         int lane, cpx<T> (&a)[NM], cd& h, cd& ht) {
-  const int n = C.n, N = C.N, S = C.S;
-  cpx<T>* pw = ws_pw<T>(ws);
-  power_table<T>(C, pw, ccast<T>(zl), lane);
-  __syncwarp();
-  run_schedule<T, F>(wc_coef<T>(C), C.meta, C.len_j, lane, pw, ws_j<T>(ws));
-  __syncwarp();
+// ---- rows of the reduced system ---------------------------------------------
+// The last row of H_z is the patch a (h_n = a . z - 1, src/homotopy.f90:228-230),
+// the same for every unit of a path. It is eliminated first, with a fixed
+// pivot: the column c of the largest |a_c| (the first such column; the
+// table header holds c, rho_j = a_j / a_c, |rho_j| <= 1, and 1/a_c). For
+// A x = r that leaves the n x n system of the equation rows over the
+// columns j != c,
+//   sum_{j != c} (A_ij - A_ic rho_j) x_j = r_i - A_ic r_n / a_c,
+// and x_c = r_n / a_c - sum_{j != c} rho_j x_j. Column c's place in the
+// reduced system is taken by column n (w) when c != n. n rows instead of
+// n + 1 put n = 16 (17 unknowns) and n = 8 into the split layouts with two
+// and four lanes per row. The pivoting differs from the reference's
+// partial pivoting over all n + 1 rows in rounding only.
 
-  const cpx<T> gamma = ccast<T>(C.gamma);
-  const cpx<T> tt = ccast<T>(t);
-  const cpx<T> gt = gamma * tt;
-  const cpx<T> omt = mkc<T>(T(1) - tt.re, -tt.im);
-  const cpx<T>* zrow = pw + N;  // z_j = pw[1*N + j]
-  // Every lane i <= n runs the same code on row i of the buffer: the
-  // Jacobian row of F^h_i (i < n) or the patch a (i = n); F^h_i follows from
-  // Euler's relation, F^h_i = (1/d_i) sum_j z_j dF^h_i/dz_j, and the patch
-  // row gives h_n = a . z - 1 (src/homotopy.f90:228-230).
-  const bool eq = lane < n;
-  const int row = lane < n ? lane : n;
-  const cpx<T>* Jr = ws_j<T>(ws) + row * S;
-  // row scale: (1 - t) for an equation row, 1 for the patch row, 0 for the
-  // lanes beyond it (their rows are all zero)
-  const cpx<T> sc = eq ? omt : (lane == n ? cone<T>() : czero<T>());
-  cpx<T> f0 = czero<T>(), f1 = czero<T>();
-#pragma unroll
-  for (int j = 0; j < NM; ++j) {
-    if (j < N) {
-      const cpx<T> jij = lds(&Jr[j]);
-      if (j & 1)
-        f1 = cfma(f1, jij, lds(&zrow[j]));
-      else
-        f0 = cfma(f0, jij, lds(&zrow[j]));
-      a[j] = sc * jij;
-    } else {
-      a[j] = czero<T>();
-    }
-  }
-  const cpx<T> f = (T)C.inv_deg * (f0 + f1);
-  // start system G_i = z_i^d - b_i w^d from the power table
-  const int dm1 = eq ? C.deg - 1 : 0;
-  const cpx<T> zd1 = lds(&pw[dm1 * N + row]);
-  const cpx<T> wd1 = lds(&pw[dm1 * N + n]);
-  const cpx<T> zi = lds(&zrow[row]);
-  const cpx<T> w = lds(&zrow[n]);
-  const cpx<T> bi = ccast<T>(C.b);
-  const cpx<T> g = zd1 * zi - (bi * wd1) * w;
-  const T dd = (T)C.deg;
-  const cpx<T> dg = eq ? (dd * gt) * zd1 : czero<T>();
-  const cpx<T> dw = eq ? (dd * (gt * bi)) * wd1 : czero<T>();
-  // dg and dw are zero outside the equation rows
-#pragma unroll
-  for (int j = 0; j < NM; ++j) {
-    if (j == lane) a[j] = a[j] + dg;
-    if (j == n) a[j] = a[j] - dw;
-  }
-  cpx<T> hh = eq ? gt * g + omt * f : (lane == n ? mkc<T>(f.re - T(1), f.im) : czero<T>());
-  cpx<T> hht = eq ? gamma * g - f : czero<T>();
-  h = ccast<double>(hh);
-  ht = ccast<double>(hht);
-}
-
-// ---- split rows (N <= 16) --------------------------------------------------
-// For systems of up to 16 unknowns S lanes share a row (S = 2 for N <= 16,
-// S = 4 for N <= 8): with RPW = 32/S rows per warp, lane L works on row
-// L % RPW and holds its columns [q*HS, (q+1)*HS), q = L / RPW. A shuffle
-// instruction then moves a different pivot-row element to each part, and
-// each lane updates, loads and holds a fraction of a row.
-
-// Sum over the S lanes that share a row (lanes i, i + RPW, ...).
+// The S lanes that share a row (lanes i, i + RPW, ...) and the rows of a
+// part: sums over them.
 template <int S, typename T>
 __device__ __forceinline__ T row_sum(T v) {
   if constexpr (S >= 4) v += __shfl_xor_sync(kFull, v, 8);
@@ -545,14 +486,27 @@ __device__ __forceinline__ T part_sum(T v) {
   return v;
 }
 
-// evaluate() for the split layout: same power table and schedule, the
-// assembly of row L % RPW over the lane's part of the columns; the Euler
-// sum adds the parts' partial sums.
+// Original column of reduced column r (r < n): r itself, except that the
+// pivot column c is replaced by column n.
+__device__ __forceinline__ int reduced_col(int r, int c, int n) { return r == c ? n : r; }
+
+// Evaluation of H(z,t) = gamma t G(z) + (1 - t) F^h(z) and its Jacobian for
+// the reduced rows (tdh_evaluate, src/homotopy.f90:188-231), in precision
+// T, with S lanes per row, HS columns each (S = 1: one lane per row, all
+// columns). Input: lane j holds z_j. Output, for lane L of row i = L % RPW
+// (i < n) and part q = L / RPW: a[jj] = H_z(i, reduced_col(q HS + jj))
+// before the patch elimination (zero beyond the n columns and for rows i
+// >= n); aic = H_z(i, c); h = h_i, ht = (H_t)_i. F^h_i is obtained from
+// row i of its Jacobian by Euler's relation for homogeneous polynomials,
+// F^h_i = (1/d_i) sum_j z_j dF^h_i/dz_j, which needs no evaluation of its
+// own. F: the schedule form of the kernel (the most power-table factors of
+// any record: 1, 2 or 3).
 template <int HS, int S, typename T, int F>
-__device__ __forceinline__ void evaluate_split(const WarpConst& C, const WarpWS& ws, cd zl, cd t,
-                                               int lane, cpx<T> (&a)[HS], cd& h, cd& ht) {
+__device__ __forceinline__ void evaluate_reduced(const WarpConst& C, const WarpWS& ws, cd zl,
+                                                 cd t, int lane, cpx<T> (&a)[HS], cpx<T>& aic,
+                                                 cd& h, cd& ht) {
   constexpr int RPW = 32 / S;
-  const int n = C.n, N = C.N, S_ = C.S;
+  const int n = C.n, N = C.N, S_ = C.S, c = C.red_c;
   cpx<T>* pw = ws_pw<T>(ws);
   power_table<T>(C, pw, ccast<T>(zl), lane);
   __syncwarp();
@@ -564,50 +518,77 @@ __device__ __forceinline__ void evaluate_split(const WarpConst& C, const WarpWS&
   const cpx<T> gt = gamma * tt;
   const cpx<T> omt = mkc<T>(T(1) - tt.re, -tt.im);
   const cpx<T>* zrow = pw + N;  // z_j = pw[1*N + j]
-  const int i = lane & (RPW - 1), j0 = (lane / RPW) * HS;
+  const int i = lane & (RPW - 1), part = lane / RPW, j0 = part * HS;
   const bool eq = i < n;
-  const int row = i < n ? i : n;
+  const int row = eq ? i : 0;
   const cpx<T>* Jr = ws_j<T>(ws) + row * S_;
-  const cpx<T> sc = eq ? omt : (i == n ? cone<T>() : czero<T>());
-  cpx<T> f0 = czero<T>(), f1 = czero<T>();
-#pragma unroll
-  for (int jj = 0; jj < HS; ++jj) {
-    const int j = j0 + jj;
-    if (j < N) {
-      const cpx<T> jij = lds(&Jr[j]);
-      if (jj & 1)
-        f1 = cfma(f1, jij, lds(&zrow[j]));
-      else
-        f0 = cfma(f0, jij, lds(&zrow[j]));
-      a[jj] = sc * jij;
-    } else {
-      a[jj] = czero<T>();
-    }
-  }
-  // the row's constants are held by lane i (WarpConst is per lane); the
-  // other parts read them from it
-  const int deg = __shfl_sync(kFull, C.deg, i);
-  const double inv_deg = __shfl_sync(kFull, C.inv_deg, i);
-  const cpx<T> f = (T)inv_deg * row_csum<S>(f0 + f1);
+  // the row's constants are held by lane i (WarpConst is per lane)
+  const int deg = (S == 1) ? C.deg : __shfl_sync(kFull, C.deg, i);
+  const double inv_deg = (S == 1) ? C.inv_deg : __shfl_sync(kFull, C.inv_deg, i);
+  const cpx<T> bi = ccast<T>((S == 1) ? C.b : shfl(C.b, i));
+  // start system G_i = z_i^d - b_i w^d from the power table, and its
+  // derivatives d_i gamma t z_i^(d-1) (column i) and -d_i gamma t b_i w^(d-1)
+  // (column n)
   const int dm1 = eq ? deg - 1 : 0;
   const cpx<T> zd1 = lds(&pw[dm1 * N + row]);
   const cpx<T> wd1 = lds(&pw[dm1 * N + n]);
   const cpx<T> zi = lds(&zrow[row]);
   const cpx<T> w = lds(&zrow[n]);
-  const cpx<T> bi = ccast<T>(shfl(C.b, i));
   const cpx<T> g = zd1 * zi - (bi * wd1) * w;
   const T dd = (T)deg;
   const cpx<T> dg = eq ? (dd * gt) * zd1 : czero<T>();
   const cpx<T> dw = eq ? (dd * (gt * bi)) * wd1 : czero<T>();
+  const cpx<T> sc = eq ? omt : czero<T>();
+  // Euler sum over the lane's columns; part 0 adds column c
+  cpx<T> f0 = czero<T>(), f1 = czero<T>();
 #pragma unroll
   for (int jj = 0; jj < HS; ++jj) {
-    if (j0 + jj == i) a[jj] = a[jj] + dg;
-    if (j0 + jj == n) a[jj] = a[jj] - dw;
+    const int r = j0 + jj;
+    if (r < n) {
+      const int o = reduced_col(r, c, n);
+      const cpx<T> jio = lds(&Jr[o]);
+      if (jj & 1)
+        f1 = cfma(f1, jio, lds(&zrow[o]));
+      else
+        f0 = cfma(f0, jio, lds(&zrow[o]));
+      cpx<T> v = sc * jio;
+      if (o == i) v = v + dg;
+      if (o == n) v = v - dw;
+      a[jj] = eq ? v : czero<T>();
+    } else {
+      a[jj] = czero<T>();
+    }
   }
-  cpx<T> hh = eq ? gt * g + omt * f : (i == n ? mkc<T>(f.re - T(1), f.im) : czero<T>());
-  cpx<T> hht = eq ? gamma * g - f : czero<T>();
+  const cpx<T> jic = lds(&Jr[c]);
+  if (part == 0) f0 = cfma(f0, jic, lds(&zrow[c]));
+  cpx<T> v = sc * jic;
+  if (c == i) v = v + dg;
+  if (c == n) v = v - dw;
+  aic = eq ? v : czero<T>();
+  const cpx<T> f = (T)inv_deg * row_csum<S>(f0 + f1);
+  const cpx<T> hh = eq ? gt * g + omt * f : czero<T>();
+  const cpx<T> hht = eq ? gamma * g - f : czero<T>();
   h = ccast<double>(hh);
   ht = ccast<double>(hht);
+}
+
+// The patch elimination of a row: a[jj] -= aic rho_o (o = reduced_col of the
+// lane's column jj; rows >= n hold zeros and stay zero).
+template <int HS, int S, typename T>
+__device__ __forceinline__ void fold_patch(const WarpConst& C, int lane, cpx<T> (&a)[HS],
+                                           cpx<T> aic) {
+  constexpr int RPW = 32 / S;
+  const int n = C.n, c = C.red_c;
+  const int j0 = (lane / RPW) * HS;
+#pragma unroll
+  for (int jj = 0; jj < HS; ++jj) {
+    const int r = j0 + jj;
+    if (r < n) {
+      const int o = reduced_col(r, c, n);
+      const cpx<T> rho = mkc<T>((T)C.rho[o][0], (T)C.rho[o][1]);
+      a[jj] = cfms(a[jj], aic, rho);
+    }
+  }
 }
 
 // ---- Gauss-Jordan elimination with partial pivoting -----------------------

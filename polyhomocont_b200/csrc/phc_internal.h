@@ -81,6 +81,15 @@ struct alignas(16) PlanHeader {
   double gamma[2];
   double b[kMaxN][2];
   double patch[kMaxN][2];
+  // the patch row's elimination (evaluate_reduced): pivot column c, the
+  // largest |a_c| (first maximum), rho_j = a_j / a_c, 1/a_c, and the patch
+  // row's absolute sum sum_j |a_j|
+  int32_t red_c;
+  int32_t pad2_[3];
+  double rho[kMaxN][2];
+  double inv_ac[2];
+  double patch_abs_sum;
+  double pad3_;
 };
 
 // Per-kernel options: the POD mirror of solve_options plus GPU knobs.
@@ -210,11 +219,12 @@ PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size, bool eval32) {
   return L;
 }
 
-// Supported register-row widths (compile-time N capacity).
+// Supported register-row widths: the compile-time capacity NM >= n of the
+// rows of the reduced n x n system (the patch row eliminated first).
 constexpr int kNMs[] = {6, 8, 12, 16, 18, 24, 32};
-inline int pick_nm(int N) {
+inline int pick_nm(int n) {
   for (int v : kNMs)
-    if (N <= v) return v;
+    if (n <= v) return v;
   return 0;
 }
 // The single-system kernels of rows up to 8 columns carry an FP32

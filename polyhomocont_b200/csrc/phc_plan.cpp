@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <complex>
 #include <map>
 #include <cstring>
 #include <numeric>
@@ -238,6 +239,7 @@ int verify_plan(const unsigned char* bytes, size_t size) {
     if (radix > (int64_t)INT32_MAX) return fail("path count");
   }
   if (H.nstart != radix) return fail("path count");
+  if (H.red_c < 0 || H.red_c >= H.N) return fail("patch pivot column");
   // extended entries: level L may use plain entries and entries of levels < L
   std::vector<char> ready(H.pw_total, 0);
   std::fill(ready.begin(), ready.begin() + H.pw_size, 1);
@@ -317,6 +319,18 @@ int validate_system(const phc_system* sys) {
   return PHC_OK;
 }
 
+// a / b by Smith's method (R. L. Smith, CACM 5 (1962) 435)
+static std::complex<double> smith_div(std::complex<double> a, std::complex<double> b) {
+  if (std::fabs(b.real()) < std::fabs(b.imag())) {
+    const double ratio = b.real() / b.imag();
+    const double den = b.real() * ratio + b.imag();
+    return {(a.real() * ratio + a.imag()) / den, (a.imag() * ratio - a.real()) / den};
+  }
+  const double ratio = b.imag() / b.real();
+  const double den = b.imag() * ratio + b.real();
+  return {(a.imag() * ratio + a.real()) / den, (a.imag() - a.real() * ratio) / den};
+}
+
 int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   int st = validate_system(sys);
   if (st != PHC_OK) return st;
@@ -357,6 +371,33 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
   for (int j = 0; j < N; ++j) {
     H.patch[j][0] = hom->patch[2 * j];
     H.patch[j][1] = hom->patch[2 * j + 1];
+  }
+  // the patch row is eliminated first on the device, pivoting on its
+  // largest entry (first maximum of |a_j|)
+  {
+    int c = 0;
+    double amax = -1.0, asum = 0.0;
+    for (int j = 0; j < N; ++j) {
+      const double m = std::hypot(H.patch[j][0], H.patch[j][1]);
+      asum += m;
+      if (m > amax) {
+        amax = m;
+        c = j;
+      }
+    }
+    if (!(amax > 0.0)) return PHC_ERR_INVALID_INPUT;  // a zero patch
+    H.red_c = c;
+    H.patch_abs_sum = asum;
+    const std::complex<double> ac(H.patch[c][0], H.patch[c][1]);
+    const std::complex<double> inv = smith_div(std::complex<double>(1.0, 0.0), ac);
+    H.inv_ac[0] = inv.real();
+    H.inv_ac[1] = inv.imag();
+    for (int j = 0; j < N; ++j) {
+      const std::complex<double> r =
+          smith_div(std::complex<double>(H.patch[j][0], H.patch[j][1]), ac);
+      H.rho[j][0] = r.real();
+      H.rho[j][1] = r.imag();
+    }
   }
 
   // Jacobian contributions per entry, in term order (eval_terms,
