@@ -1,5 +1,6 @@
 // Instantiation unit of the tracking kernel for register rows of 8
-// complex entries (systems with N = n + 1 <= 8 unknowns).
+// complex entries (systems of n <= 8 equations: the rows of the reduced
+// system, the patch row eliminated first).
 #include "phc_track.cuh"
 
 PHC_DEFINE_NM(8)
