@@ -202,7 +202,7 @@ int device_sms(int device) {
 }
 
 int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, LaunchCfg* cfg) {
-  cfg->nm = pick_nm(hp.n);  // n rows once the patch row is eliminated
+  cfg->nm = pick_nm(eliminated_rows(hp.n));
   if (cfg->nm == 0) {
     set_last_error("more than 32 unknowns");
     return PHC_ERR_UNSUPPORTED;

@@ -317,7 +317,7 @@ struct WarpConst {
   const cf* coeff;
   const uint2* meta;
   const double (*patch)[2];
-  int red_c;                   // pivot column of the patch row (see evaluate_reduced)
+  int red_c;                   // pivot column of the patch row (see evaluate_rows_of)
   const double (*rho)[2];      // rho_j = a_j / a_c
 };
 
@@ -452,19 +452,22 @@ template <> __device__ __forceinline__ const cf* plan_coef<float>(const unsigned
   return reinterpret_cast<const cf*>(pb + off_f);
 }
 
-// ---- rows of the reduced system ---------------------------------------------
+// ---- rows of the system, and the reduced system -----------------------------
 // The last row of H_z is the patch a (h_n = a . z - 1, src/homotopy.f90:228-230),
-// the same for every unit of a path. It is eliminated first, with a fixed
-// pivot: the column c of the largest |a_c| (the first such column; the
-// table header holds c, rho_j = a_j / a_c, |rho_j| <= 1, and 1/a_c). For
+// the same for every unit of a path. Normally it is one of the N rows the
+// elimination pivots over, as in the reference's LU. For n = 8 and n = 16
+// (the table header's `reduce`) it is eliminated first instead, with a
+// fixed pivot: the column c of the largest |a_c| (the first such column;
+// the header holds c, rho_j = a_j / a_c, |rho_j| <= 1, and 1/a_c). For
 // A x = r that leaves the n x n system of the equation rows over the
 // columns j != c,
 //   sum_{j != c} (A_ij - A_ic rho_j) x_j = r_i - A_ic r_n / a_c,
 // and x_c = r_n / a_c - sum_{j != c} rho_j x_j. Column c's place in the
 // reduced system is taken by column n (w) when c != n. n rows instead of
 // n + 1 put n = 16 (17 unknowns) and n = 8 into the split layouts with two
-// and four lanes per row. The pivoting differs from the reference's
-// partial pivoting over all n + 1 rows in rounding only.
+// and four lanes per row. Its pivoting differs from the reference's
+// partial pivoting over all n + 1 rows, which changes rounding; for the
+// other sizes, whose layout it would not change, the patch stays a row.
 
 // The S lanes that share a row (lanes i, i + RPW, ...) and the rows of a
 // part: sums over them.
@@ -490,21 +493,26 @@ __device__ __forceinline__ T part_sum(T v) {
 // pivot column c is replaced by column n.
 __device__ __forceinline__ int reduced_col(int r, int c, int n) { return r == c ? n : r; }
 
-// Evaluation of H(z,t) = gamma t G(z) + (1 - t) F^h(z) and its Jacobian for
-// the reduced rows (tdh_evaluate, src/homotopy.f90:188-231), in precision
-// T, with S lanes per row, HS columns each (S = 1: one lane per row, all
-// columns). Input: lane j holds z_j. Output, for lane L of row i = L % RPW
-// (i < n) and part q = L / RPW: a[jj] = H_z(i, reduced_col(q HS + jj))
-// before the patch elimination (zero beyond the n columns and for rows i
-// >= n); aic = H_z(i, c); h = h_i, ht = (H_t)_i. F^h_i is obtained from
-// row i of its Jacobian by Euler's relation for homogeneous polynomials,
+// Evaluation of H(z,t) = gamma t G(z) + (1 - t) F^h(z) and its Jacobian
+// (tdh_evaluate, src/homotopy.f90:188-231) in precision T, with S lanes per
+// row and HS columns each (S = 1: one lane per row, all columns). Input:
+// lane j holds z_j. Output, for lane L of row i = L % RPW and part
+// q = L / RPW:
+//   reduce = 0: rows i <= n of H_z (row n the patch) over the N columns:
+//     a[jj] = H_z(i, q HS + jj), h = h_i, ht = (H_t)_i;
+//   reduce = 1: the n equation rows over the reduced columns, before the
+//     patch elimination: a[jj] = H_z(i, reduced_col(q HS + jj)),
+//     aic = H_z(i, c);
+// zero beyond the rows and columns. F^h_i is obtained from row i of its
+// Jacobian by Euler's relation for homogeneous polynomials,
 // F^h_i = (1/d_i) sum_j z_j dF^h_i/dz_j, which needs no evaluation of its
-// own. F: the schedule form of the kernel (the most power-table factors of
-// any record: 1, 2 or 3).
+// own; the patch row's h_n = a . z - 1 follows the same way (its buffer
+// row holds a, "degree" 1). F: the schedule form of the kernel (the most
+// power-table factors of any record: 1, 2 or 3).
 template <int HS, int S, typename T, int F>
-__device__ __forceinline__ void evaluate_reduced(const WarpConst& C, const WarpWS& ws, cd zl,
-                                                 cd t, int lane, cpx<T> (&a)[HS], cpx<T>& aic,
-                                                 cd& h, cd& ht) {
+__device__ __forceinline__ void evaluate_rows_of(const WarpConst& C, const WarpWS& ws, cd zl,
+                                                 cd t, int lane, bool reduce, cpx<T> (&a)[HS],
+                                                 cpx<T>& aic, cd& h, cd& ht) {
   constexpr int RPW = 32 / S;
   const int n = C.n, N = C.N, S_ = C.S, c = C.red_c;
   cpx<T>* pw = ws_pw<T>(ws);
@@ -520,9 +528,12 @@ __device__ __forceinline__ void evaluate_reduced(const WarpConst& C, const WarpW
   const cpx<T>* zrow = pw + N;  // z_j = pw[1*N + j]
   const int i = lane & (RPW - 1), part = lane / RPW, j0 = part * HS;
   const bool eq = i < n;
-  const int row = eq ? i : 0;
+  const bool patch = !reduce && i == n;
+  const int row = eq ? i : n;  // rows beyond the system read the patch row (scale 0)
+  const int ncols = reduce ? n : N;
   const cpx<T>* Jr = ws_j<T>(ws) + row * S_;
-  // the row's constants are held by lane i (WarpConst is per lane)
+  // the row's constants are held by lane i (WarpConst is per lane; lane n
+  // has degree 1 and 1/d = 1, for the patch row)
   const int deg = (S == 1) ? C.deg : __shfl_sync(kFull, C.deg, i);
   const double inv_deg = (S == 1) ? C.inv_deg : __shfl_sync(kFull, C.inv_deg, i);
   const cpx<T> bi = ccast<T>((S == 1) ? C.b : shfl(C.b, i));
@@ -538,14 +549,17 @@ __device__ __forceinline__ void evaluate_reduced(const WarpConst& C, const WarpW
   const T dd = (T)deg;
   const cpx<T> dg = eq ? (dd * gt) * zd1 : czero<T>();
   const cpx<T> dw = eq ? (dd * (gt * bi)) * wd1 : czero<T>();
-  const cpx<T> sc = eq ? omt : czero<T>();
-  // Euler sum over the lane's columns; part 0 adds column c
+  // row scale: (1 - t) for an equation row, 1 for the patch row, 0 beyond
+  const cpx<T> sc = eq ? omt : (patch ? cone<T>() : czero<T>());
+  const bool live = eq || patch;
+  // Euler sum over the lane's columns; in the reduced system part 0 adds
+  // column c
   cpx<T> f0 = czero<T>(), f1 = czero<T>();
 #pragma unroll
   for (int jj = 0; jj < HS; ++jj) {
     const int r = j0 + jj;
-    if (r < n) {
-      const int o = reduced_col(r, c, n);
+    if (r < ncols) {
+      const int o = reduce ? reduced_col(r, c, n) : r;
       const cpx<T> jio = lds(&Jr[o]);
       if (jj & 1)
         f1 = cfma(f1, jio, lds(&zrow[o]));
@@ -554,19 +568,22 @@ __device__ __forceinline__ void evaluate_reduced(const WarpConst& C, const WarpW
       cpx<T> v = sc * jio;
       if (o == i) v = v + dg;
       if (o == n) v = v - dw;
-      a[jj] = eq ? v : czero<T>();
+      a[jj] = live ? v : czero<T>();
     } else {
       a[jj] = czero<T>();
     }
   }
-  const cpx<T> jic = lds(&Jr[c]);
-  if (part == 0) f0 = cfma(f0, jic, lds(&zrow[c]));
-  cpx<T> v = sc * jic;
-  if (c == i) v = v + dg;
-  if (c == n) v = v - dw;
-  aic = eq ? v : czero<T>();
+  aic = czero<T>();
+  if (reduce) {
+    const cpx<T> jic = lds(&Jr[c]);
+    if (part == 0) f0 = cfma(f0, jic, lds(&zrow[c]));
+    cpx<T> v = sc * jic;
+    if (c == i) v = v + dg;
+    if (c == n) v = v - dw;
+    aic = eq ? v : czero<T>();
+  }
   const cpx<T> f = (T)inv_deg * row_csum<S>(f0 + f1);
-  const cpx<T> hh = eq ? gt * g + omt * f : czero<T>();
+  const cpx<T> hh = eq ? gt * g + omt * f : (patch ? mkc<T>(f.re - T(1), f.im) : czero<T>());
   const cpx<T> hht = eq ? gamma * g - f : czero<T>();
   h = ccast<double>(hh);
   ht = ccast<double>(hht);

@@ -81,11 +81,12 @@ struct alignas(16) PlanHeader {
   double gamma[2];
   double b[kMaxN][2];
   double patch[kMaxN][2];
-  // the patch row's elimination (evaluate_reduced): pivot column c, the
-  // largest |a_c| (first maximum), rho_j = a_j / a_c, 1/a_c, and the patch
-  // row's absolute sum sum_j |a_j|
+  // the patch row eliminated first (evaluate_rows_of; reduce = 1 for n = 8
+  // and n = 16): pivot column c, the largest |a_c| (first maximum),
+  // rho_j = a_j / a_c, 1/a_c, and the patch row's absolute sum sum_j |a_j|
+  int32_t reduce;
   int32_t red_c;
-  int32_t pad2_[3];
+  int32_t pad2_[2];
   double rho[kMaxN][2];
   double inv_ac[2];
   double patch_abs_sum;
@@ -219,14 +220,20 @@ PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size, bool eval32) {
   return L;
 }
 
-// Supported register-row widths: the compile-time capacity NM >= n of the
-// rows of the reduced n x n system (the patch row eliminated first).
+// Supported register-row widths: the compile-time capacity NM of the rows
+// of the eliminated system, N = n + 1 rows, or n when the patch row is
+// eliminated first.
 constexpr int kNMs[] = {6, 8, 12, 16, 18, 24, 32};
-inline int pick_nm(int n) {
+inline int pick_nm(int rows) {
   for (int v : kNMs)
-    if (n <= v) return v;
+    if (rows <= v) return v;
   return 0;
 }
+// The patch row is eliminated first where that moves the system into a
+// layout with more lanes per row: 9 and 17 unknowns have 8 and 16 equation
+// rows, which fit the four- and two-lane layouts (rows of up to 8 and 16).
+PHC_HD constexpr bool reduce_patch_row(int n) { return n == 8 || n == 16; }
+PHC_HD constexpr int eliminated_rows(int n) { return reduce_patch_row(n) ? n : n + 1; }
 // The single-system kernels of rows up to 8 columns carry an FP32
 // evaluation for the mixed predictor; every other kernel evaluates in FP64.
 PHC_HD constexpr bool kernel_eval32(int nm, int precision) {

@@ -240,6 +240,7 @@ int verify_plan(const unsigned char* bytes, size_t size) {
   }
   if (H.nstart != radix) return fail("path count");
   if (H.red_c < 0 || H.red_c >= H.N) return fail("patch pivot column");
+  if (H.reduce != (reduce_patch_row(H.n) ? 1 : 0)) return fail("patch row elimination");
   // extended entries: level L may use plain entries and entries of levels < L
   std::vector<char> ready(H.pw_total, 0);
   std::fill(ready.begin(), ready.begin() + H.pw_size, 1);
@@ -386,6 +387,7 @@ int build_plan(const phc_system* sys, const phc_homotopy* hom, HostPlan* out) {
       }
     }
     if (!(amax > 0.0)) return PHC_ERR_INVALID_INPUT;  // a zero patch
+    H.reduce = reduce_patch_row(n) ? 1 : 0;
     H.red_c = c;
     H.patch_abs_sum = asum;
     const std::complex<double> ac(H.patch[c][0], H.patch[c][1]);

@@ -60,7 +60,7 @@ constexpr int kCondChunk = 4;
 // UK_COND eliminates against the unit vectors e_c0 .. e_c0+3 (cond1,
 // src/linalg.f90:135-174); the state machine runs one such unit per chunk.
 // Rows of up to 16 columns use the split layout (two lanes per row, half
-// a row each: evaluate_reduced, gauss_jordan_split); wider rows one lane per
+// a row each: evaluate_rows_of, gauss_jordan_split); wider rows one lane per
 // row.
 // Workspace pointers of a warp inside its shared-memory region. The FP32
 // power table and Jacobian buffer exist only in kernels that carry the FP32
@@ -91,20 +91,21 @@ struct RowLayout {
 
 template <int NM, typename T, int F>
 __device__ __forceinline__ void evaluate_rows(const WarpConst& C, const WarpWS& ws, cd z, cd t,
-                                              int lane, cpx<T> (&a)[RowLayout<NM>::kRegs],
-                                              cpx<T>& aic, cd& h, cd& ht) {
-  evaluate_reduced<RowLayout<NM>::kRegs, RowLayout<NM>::kLanes, T, F>(C, ws, z, t, lane, a, aic,
-                                                                      h, ht);
+                                              int lane, bool reduce,
+                                              cpx<T> (&a)[RowLayout<NM>::kRegs], cpx<T>& aic,
+                                              cd& h, cd& ht) {
+  evaluate_rows_of<RowLayout<NM>::kRegs, RowLayout<NM>::kLanes, T, F>(C, ws, z, t, lane, reduce,
+                                                                      a, aic, h, ht);
 }
 
 template <int NM, int R, typename T>
-__device__ __forceinline__ bool eliminate(cpx<T> (&a)[RowLayout<NM>::kRegs], cpx<T> (&r)[R], int n,
-                                          int lane, int* piv) {
+__device__ __forceinline__ bool eliminate(cpx<T> (&a)[RowLayout<NM>::kRegs], cpx<T> (&r)[R],
+                                          int rows, int lane, int* piv) {
   if constexpr (RowLayout<NM>::kSplit)
-    return gauss_jordan_split<RowLayout<NM>::kRegs, RowLayout<NM>::kLanes, R, T>(a, r, n, lane,
+    return gauss_jordan_split<RowLayout<NM>::kRegs, RowLayout<NM>::kLanes, R, T>(a, r, rows, lane,
                                                                                 piv);
   else
-    return gauss_jordan<NM, R, T>(a, r, n, lane, piv);
+    return gauss_jordan<NM, R, T>(a, r, rows, lane, piv);
 }
 
 // h_n = a . z - 1, the patch row of H (src/homotopy.f90:228-230), on every
@@ -116,14 +117,20 @@ __device__ __forceinline__ cd patch_residual(const WarpConst& C, cd z, int lane)
   return mkc<double>(s.re - 1.0, s.im);
 }
 
-// The solution x of the full system from the reduced one (see
-// evaluate_reduced): lane j receives x_j. y: the eliminated right-hand
-// side (reduced component r in lane piv[r]); rn: the patch row's
-// right-hand side.
+// The solution x of the full system (lane j receives x_j) from the
+// eliminated right-hand side y (component r of the eliminated system in
+// lane piv[r]). With the patch row eliminated first (see
+// evaluate_rows_of), rn is its right-hand side and x_c follows from the
+// others.
 template <typename T>
 __device__ __forceinline__ cd full_solution(const PlanHeader& P, const WarpConst& C,
-                                            const WarpWS& ws, cpx<T> y, cd rn, int lane) {
+                                            const WarpWS& ws, bool reduce, cpx<T> y, cd rn,
+                                            int lane) {
   const int n = C.n, N = C.N, c = C.red_c;
+  if (!reduce) {
+    const cpx<T> yj = shfl(y, ws.piv[lane < N ? lane : 0]);
+    return (lane < N) ? ccast<double>(yj) : czero<double>();
+  }
   const bool own = lane < N && lane != c;
   const int src = (lane == n) ? c : lane;  // reduced column of unknown `lane`
   const cpx<T> yj = shfl(y, ws.piv[own ? src : 0]);
@@ -137,9 +144,9 @@ __device__ __forceinline__ cd full_solution(const PlanHeader& P, const WarpConst
 // The unit reads the system's constants and its workspace pointers from
 // shared memory itself (tbl: the staged table, wbase: the warp's
 // workspace), so that nothing of them stays live in registers between
-// units. It works on the reduced system of the n equation rows (the patch
-// row eliminated first, see evaluate_reduced) and returns the solution of
-// the full one.
+// units. With the patch row eliminated first (the header's `reduce`) it
+// works on the n x n reduced system and returns the solution of the full
+// one.
 template <int NM, bool MIXED, bool EVAL32, int F>
 __device__ __forceinline__ void run_unit(const unsigned char* tbl, unsigned char* wbase, int kind,
                                          int prec, int c0, cd zin, cd t, cd dt, int lane,
@@ -150,88 +157,125 @@ __device__ __forceinline__ void run_unit(const unsigned char* tbl, unsigned char
   const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(tbl);
   const WarpConst C = load_warp_const(P, tbl, lane);
   const WarpWS ws = warp_workspace<EVAL32>(P, wbase);
-  const int n = C.n, c = C.red_c;
-  // the row this lane works on (rows >= n hold zeros)
+  const int n = C.n, N = C.N, c = C.red_c;
+  const bool reduce = P.reduce != 0;
+  const int rows = reduce ? n : N;  // rows of the eliminated system
+  // the row this lane works on (rows >= `rows` hold zeros), and whether it
+  // reports the row (part 0)
   const int row = lane & (L::kRows - 1);
+  const bool owner = lane < L::kRows;
   cd h, ht;
   cpx<float> as[RW];
   cpx<float> rs32;
-  cd rn = czero<double>();  // the patch row's right-hand side
+  cd rn = czero<double>();  // the patch row's right-hand side (reduced system)
   if (!MIXED || !EVAL32 || prec != 2) {
     cpx<double> a[RW];
     cd aic;
-    evaluate_rows<NM, double, F>(C, ws, zin, t, lane, a, aic, h, ht);
+    evaluate_rows<NM, double, F>(C, ws, zin, t, lane, reduce, a, aic, h, ht);
     if (kind == UK_BACKERR) {
       // backward_error, src/endgame.f90:269-285: ||H(z,0)|| and the maximum
       // absolute row sum of H_z, over the n equation rows and the patch row
       double rsum = 0.0;
 #pragma unroll
       for (int j = 0; j < RW; ++j) rsum += cabs(a[j]);
-      rsum = row_sum<S>(rsum) + cabs(aic);
-      const double hn = cabs(patch_residual(C, zin, lane));
-      u.a1 = fmax(warp_max_nonneg(row < n ? cabs(h) : 0.0), hn);
-      u.a2 = fmax(warp_max_nonneg(row < n ? rsum : 0.0), P.patch_abs_sum);
+      rsum = row_sum<S>(rsum);
+      if (reduce) {
+        rsum += cabs(aic);
+        const double hn = cabs(patch_residual(C, zin, lane));
+        u.a1 = fmax(warp_max_nonneg(row < n ? cabs(h) : 0.0), hn);
+        u.a2 = fmax(warp_max_nonneg(row < n ? rsum : 0.0), P.patch_abs_sum);
+      } else {
+        u.a1 = warp_max_nonneg(row < N ? cabs(h) : 0.0);
+        u.a2 = warp_max_nonneg(row < N ? rsum : 0.0);
+      }
       u.ok = true;
       return;
     }
     if (kind == UK_COND) {
       u.h = h;
       if (c0 == 0) {
-        // ||A||_1: the largest column sum over the n equation rows and the
-        // patch row; every column but c is one of the lane's columns
-        const int j0 = (lane / L::kRows) * RW;
-        double anorm = 0.0;
+        // ||A||_1: the largest column sum over all N rows
+        if (reduce) {
+          // every column but c is one of the lane's columns; the patch row
+          // adds |a_o|
+          const int j0 = (lane / L::kRows) * RW;
+          double anorm = 0.0;
 #pragma unroll
-        for (int jj = 0; jj < RW; ++jj) {
-          const int r = j0 + jj;
-          const double cs = part_sum<S>(row < n ? cabs(a[jj]) : 0.0);
-          if (r < n) {
-            const int o = reduced_col(r, c, n);
-            anorm = fmax(anorm, cs + hypot(C.patch[o][0], C.patch[o][1]));
+          for (int jj = 0; jj < RW; ++jj) {
+            const int r = j0 + jj;
+            const double cs = part_sum<S>(row < n ? cabs(a[jj]) : 0.0);
+            if (r < n) {
+              const int o = reduced_col(r, c, n);
+              anorm = fmax(anorm, cs + hypot(C.patch[o][0], C.patch[o][1]));
+            }
           }
-        }
-        const double csc = part_sum<S>(row < n ? cabs(aic) : 0.0);
-        anorm = fmax(anorm, csc + hypot(C.patch[c][0], C.patch[c][1]));
-        u.a1 = warp_max_nonneg(anorm);
-      }
-      fold_patch<RW, S, double>(C, lane, a, aic);
-      // right-hand sides e_col, col = c0 .. c0+3 (unknowns 0..N-1); the
-      // patch row's is 1 for col = n
-      const cd inv_ac = mkc<double>(P.inv_ac[0], P.inv_ac[1]);
-      cd r[kCondChunk];
+          const double csc = part_sum<S>(row < n ? cabs(aic) : 0.0);
+          anorm = fmax(anorm, csc + hypot(C.patch[c][0], C.patch[c][1]));
+          u.a1 = warp_max_nonneg(anorm);
+        } else {
+          double anorm = 0.0;
 #pragma unroll
-      for (int q = 0; q < kCondChunk; ++q) {
-        const cd rq = (row == c0 + q && row < n) ? cone<double>() : czero<double>();
-        r[q] = (c0 + q == n) ? rq - aic * inv_ac : rq;
+          for (int j = 0; j < RW; ++j) {
+            if constexpr (L::kSplit)
+              anorm = fmax(anorm, part_sum<S>(row < N ? cabs(a[j]) : 0.0));
+            else if (j < N)
+              anorm = fmax(anorm, warp_sum(row < N ? cabs(a[j]) : 0.0));
+          }
+          if constexpr (L::kSplit) anorm = warp_max_nonneg(anorm);
+          u.a1 = anorm;
+        }
       }
-      if (!eliminate<NM, kCondChunk, double>(a, r, n, lane, ws.piv)) {
+      // right-hand sides e_col, col = c0 .. c0+3 (unknowns 0..N-1); in the
+      // reduced system the patch row's is 1 for col = n
+      cd r[kCondChunk];
+      if (reduce) {
+        fold_patch<RW, S, double>(C, lane, a, aic);
+        const cd inv_ac = mkc<double>(P.inv_ac[0], P.inv_ac[1]);
+#pragma unroll
+        for (int q = 0; q < kCondChunk; ++q) {
+          const cd rq = (row == c0 + q && row < n) ? cone<double>() : czero<double>();
+          r[q] = (c0 + q == n) ? rq - aic * inv_ac : rq;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < kCondChunk; ++q)
+          r[q] = (row == c0 + q) ? cone<double>() : czero<double>();
+      }
+      if (!eliminate<NM, kCondChunk, double>(a, r, rows, lane, ws.piv)) {
         u.ok = false;  // cond1 of an exactly singular matrix
         return;
       }
       double ainv = 0.0;
 #pragma unroll
       for (int q = 0; q < kCondChunk; ++q) {
-        if (c0 + q < C.N) {
-          const cd rnq = (c0 + q == n) ? cone<double>() : czero<double>();
-          const cd x = full_solution<double>(P, C, ws, r[q], rnq, lane);
-          ainv = fmax(ainv, warp_sum(lane < C.N ? cabs(x) : 0.0));
+        if (c0 + q < N) {
+          if (reduce) {
+            const cd rnq = (c0 + q == n) ? cone<double>() : czero<double>();
+            const cd x = full_solution<double>(P, C, ws, true, r[q], rnq, lane);
+            ainv = fmax(ainv, warp_sum(lane < N ? cabs(x) : 0.0));
+          } else {
+            // the column sum is the same in pivot order
+            ainv = fmax(ainv, warp_sum(owner && row < N ? cabs(r[q]) : 0.0));
+          }
         }
       }
       u.a2 = ainv;
       u.ok = true;
       return;
     }
-    fold_patch<RW, S, double>(C, lane, a, aic);
     cd r0 = (kind == UK_TANGENT) ? -(ht * dt) : -h;
-    if (kind != UK_TANGENT) {  // H_t of the patch row is zero
-      rn = -patch_residual(C, zin, lane);
-      r0 = r0 - aic * (rn * mkc<double>(P.inv_ac[0], P.inv_ac[1]));
+    if (reduce) {
+      fold_patch<RW, S, double>(C, lane, a, aic);
+      if (kind != UK_TANGENT) {  // H_t of the patch row is zero
+        rn = -patch_residual(C, zin, lane);
+        r0 = r0 - aic * (rn * mkc<double>(P.inv_ac[0], P.inv_ac[1]));
+      }
     }
     if (!MIXED || prec == 0) {
       cd r[1] = {r0};
-      u.ok = eliminate<NM, 1, double>(a, r, n, lane, ws.piv);
+      u.ok = eliminate<NM, 1, double>(a, r, rows, lane, ws.piv);
       if (!u.ok) return;
-      u.x = full_solution<double>(P, C, ws, r[0], rn, lane);
+      u.x = full_solution<double>(P, C, ws, reduce, r[0], rn, lane);
       return;
     }
     // FP64 evaluation, FP32 elimination
@@ -241,17 +285,18 @@ __device__ __forceinline__ void run_unit(const unsigned char* tbl, unsigned char
       rs32 = ccast<float>(r0);
     }
   } else if constexpr (MIXED && EVAL32) {
-    // FP32 evaluation (the predictor: its patch right-hand side is zero)
+    // FP32 evaluation (the predictor: the patch row's right-hand side is
+    // zero)
     cpx<float> aic;
-    evaluate_rows<NM, float, F>(C, ws, zin, t, lane, as, aic, h, ht);
-    fold_patch<RW, S, float>(C, lane, as, aic);
+    evaluate_rows<NM, float, F>(C, ws, zin, t, lane, reduce, as, aic, h, ht);
+    if (reduce) fold_patch<RW, S, float>(C, lane, as, aic);
     rs32 = ccast<float>(-(ht * dt));
   }
   if constexpr (MIXED) {
     cpx<float> r[1] = {rs32};
-    u.ok = eliminate<NM, 1, float>(as, r, n, lane, ws.piv);
+    u.ok = eliminate<NM, 1, float>(as, r, rows, lane, ws.piv);
     if (!u.ok) return;
-    u.x = full_solution<float>(P, C, ws, r[0], rn, lane);
+    u.x = full_solution<float>(P, C, ws, reduce, r[0], rn, lane);
   }
 }
 

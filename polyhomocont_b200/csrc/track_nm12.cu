@@ -1,6 +1,7 @@
 // Instantiation unit of the tracking kernel for register rows of 12
-// complex entries (systems of n <= 12 equations: the rows of the reduced
-// system, the patch row eliminated first).
+// complex entries (systems whose eliminated rows -- the N = n + 1 rows, or
+// the n equation rows when the patch row is eliminated first -- number at
+// most 12).
 #include "phc_track.cuh"
 
 PHC_DEFINE_NM(12)

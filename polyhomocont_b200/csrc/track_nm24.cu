@@ -1,6 +1,7 @@
 // Instantiation unit of the tracking kernel for register rows of 24
-// complex entries (systems of n <= 24 equations: the rows of the reduced
-// system, the patch row eliminated first).
+// complex entries (systems whose eliminated rows -- the N = n + 1 rows, or
+// the n equation rows when the patch row is eliminated first -- number at
+// most 24).
 #include "phc_track.cuh"
 
 PHC_DEFINE_NM(24)
