@@ -2,8 +2,8 @@
 solve() on every benchmark configuration, path by path, in both precision
 modes:
 
-  - the serving stream: the first 64 systems of the request stream (n from
-    2 to 8, degrees 2 and 3, 6-30 monomials per equation), each a whole
+  - the serving stream: the first 10 systems of each size n = 2..8 of the
+    request stream (degrees 2 and 3, 6-30 monomials per equation), each a whole
     solve() (src/solve.f90:154-215) on both sides, bookkeeping included,
     once solved one by one and once submitted together to the serving loop;
   - n = 10 with 1024 paths: every path, and the whole solve();
@@ -32,7 +32,7 @@ pytestmark = pytest.mark.gpu
 
 PRECISIONS = [P.PHC_PREC_FP64, P.PHC_PREC_MIXED]
 NT = os.cpu_count() or 4
-STREAM_SYSTEMS = 64
+STREAM_PER_SIZE = 10
 CFG5_WINDOWS = 8
 CFG5_WINDOW = 128
 PATH_KEYS = ("status", "winding_number", "endgame_status", "at_infinity", "singular",
@@ -46,14 +46,26 @@ def need_gpu():
         pytest.fail("GPU tests need a CUDA device")
 
 
+def stream_indices(per_size=STREAM_PER_SIZE):
+    """The first per_size systems of each size n = 2..8 of the stream."""
+    picked = {n: [] for n in range(2, 9)}
+    i = 0
+    while any(len(v) < per_size for v in picked.values()):
+        n, _ = W.stream_system(i)
+        if len(picked[n]) < per_size:
+            picked[n].append(i)
+        i += 1
+    return sorted(j for v in picked.values() for j in v)
+
+
 @pytest.fixture(scope="module")
 def stream_refs(orc):
     out = []
-    for i in range(STREAM_SYSTEMS):
+    for i in stream_indices():
         n, eqs = W.stream_system(i)
         ref, st = orc.solve(W.build(orc.SparseSystem, n, eqs), nthreads=NT)
         assert st == 0
-        out.append((n, eqs, ref))
+        out.append((i, n, eqs, ref))
     return out
 
 
@@ -61,7 +73,7 @@ def stream_refs(orc):
 def test_serving_stream_systems(stream_refs, precision):
     g = P.default_gpu_options(precision=precision)
     sizes = set()
-    for i, (n, eqs, ref) in enumerate(stream_refs):
+    for i, n, eqs, ref in stream_refs:
         got, st = P.solve(W.build(P.SparseSystem, n, eqs), gpu=g)
         assert st == 0, i
         try:
@@ -81,11 +93,11 @@ def test_serving_stream_through_the_server(stream_refs, precision):
                    gpu=P.default_gpu_options(precision=precision))
     try:
         tickets = []
-        for n, eqs, ref in stream_refs:
+        for i, n, eqs, ref in stream_refs:
             t, st = srv.submit(W.build(P.SparseSystem, n, eqs))
             assert st == 0
             tickets.append(t)
-        for i, ((n, eqs, ref), t) in enumerate(zip(stream_refs, tickets)):
+        for (i, n, eqs, ref), t in zip(stream_refs, tickets):
             assert srv.wait(t, 600000) == 0
             got, st, _ = srv.result(t)
             assert st == 0, i
@@ -177,3 +189,9 @@ def test_large_system_windows(cfg5_ref, precision):
         d = np.max(np.abs(xg[fin] - xr[fin]), axis=1) / np.maximum(
             1.0, np.max(np.abs(xr[fin]), axis=1))
         assert d.max() <= TOL_REGULAR, (k0, d.max())
+
+
+def test_stream_indices_cover_every_size():
+    idx = stream_indices()
+    assert len(idx) == 7 * STREAM_PER_SIZE
+    assert {W.stream_system(i)[0] for i in idx} == set(range(2, 9))
