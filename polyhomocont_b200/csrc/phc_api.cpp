@@ -201,8 +201,14 @@ int device_sms(int device) {
   return v;
 }
 
-int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, LaunchCfg* cfg) {
+bool use_lean(int64_t paths, int device) {
+  return paths > (int64_t)2 * kLeanPathsPerSm * device_sms(device);
+}
+
+int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, int64_t paths,
+                   LaunchCfg* cfg) {
   cfg->nm = pick_nm(eliminated_rows(hp.n));
+  cfg->lean = use_lean(paths, device) ? 1 : 0;
   if (cfg->nm == 0) {
     set_last_error("more than 32 unknowns");
     return PHC_ERR_UNSUPPORTED;
@@ -211,7 +217,7 @@ int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, Lau
   cfg->fac = hp.max_fac <= 1 ? 1 : (hp.max_fac == 2 ? 2 : 3);
   cfg->persistent = (g.schedule == PHC_SCHED_PERSISTENT) ? 1 : 0;
   int tw = 4, tc = 1;
-  tuned_launch(device, cfg->precision, cfg->persistent, cfg->nm, &tw, &tc);
+  tuned_launch(device, cfg->precision, cfg->persistent, cfg->nm, cfg->lean, &tw, &tc);
   cfg->chunk = g.chunk > 0 ? g.chunk : tc;
   cfg->eval32 = kernel_eval32(cfg->nm, cfg->precision) ? 1 : 0;
   cfg->ws_bytes = ws_layout(hp.n, hp.S, hp.pw_size, cfg->eval32 != 0).bytes;
@@ -221,7 +227,7 @@ int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, Lau
   cfg->plan_bytes = plan_bytes;
   const int smax = device_smem_optin(device);
   int warps = g.warps_per_block > 0 ? g.warps_per_block : tw;
-  warps = std::min(std::max(warps, 1), max_warps_per_block(cfg->nm));
+  warps = std::min(std::max(warps, 1), max_warps_per_block(cfg->nm, cfg->lean != 0));
   while (warps > 1 && plan_bytes + warps * cfg->ws_bytes > smax) --warps;
   if (plan_bytes + warps * cfg->ws_bytes > smax) {
     set_last_error("system table does not fit in shared memory");
@@ -297,7 +303,7 @@ static int run_paths_sync(const HostPlan& hp, const phc_solve_options& so,
     W.ready = true;
   }
   LaunchCfg cfg;
-  st = resolve_launch(hp, g, g.device, &cfg);
+  st = resolve_launch(hp, g, g.device, count, &cfg);
   if (st != PHC_OK) return st;
   const size_t nout = (size_t)count * sizeof(phc_path_out);
   const size_t nz = (size_t)count * hp.N * 2 * sizeof(double);
@@ -900,7 +906,7 @@ int32_t phc_plan_create(const phc_system* sys, const phc_homotopy* hom,
   if (st != PHC_OK) return st;
   p->device = g.device;
   PHC_CUDA(cudaSetDevice(g.device));
-  st = resolve_launch(p->hp, g, g.device, &p->cfg);
+  st = resolve_launch(p->hp, g, g.device, p->hp.nstart, &p->cfg);
   if (st != PHC_OK) return st;
   p->kopts = make_kopts(so, g);
   PHC_CUDA(cudaMalloc(&p->d_plan, p->hp.bytes.size() + 16));

@@ -455,19 +455,18 @@ template <> __device__ __forceinline__ const cf* plan_coef<float>(const unsigned
 // ---- rows of the system, and the reduced system -----------------------------
 // The last row of H_z is the patch a (h_n = a . z - 1, src/homotopy.f90:228-230),
 // the same for every unit of a path. Normally it is one of the N rows the
-// elimination pivots over, as in the reference's LU. For n = 8 and n = 16
-// (the table header's `reduce`) it is eliminated first instead, with a
+// elimination pivots over, as in the reference's LU. For n = 16 (the table
+// header's `reduce`) it is eliminated first instead, with a
 // fixed pivot: the column c of the largest |a_c| (the first such column;
 // the header holds c, rho_j = a_j / a_c, |rho_j| <= 1, and 1/a_c). For
 // A x = r that leaves the n x n system of the equation rows over the
 // columns j != c,
 //   sum_{j != c} (A_ij - A_ic rho_j) x_j = r_i - A_ic r_n / a_c,
 // and x_c = r_n / a_c - sum_{j != c} rho_j x_j. Column c's place in the
-// reduced system is taken by column n (w) when c != n. n rows instead of
-// n + 1 put n = 16 (17 unknowns) and n = 8 into the split layouts with two
-// and four lanes per row. Its pivoting differs from the reference's
-// partial pivoting over all n + 1 rows, which changes rounding; for the
-// other sizes, whose layout it would not change, the patch stays a row.
+// reduced system is taken by column n (w) when c != n. 16 rows instead of
+// 17 put n = 16 into the split layout with two lanes per row. Its pivoting
+// differs from the reference's partial pivoting over all n + 1 rows, which
+// changes rounding; for the other sizes the patch stays a row.
 
 // The S lanes that share a row (lanes i, i + RPW, ...) and the rows of a
 // part: sums over them.

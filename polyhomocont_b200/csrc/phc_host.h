@@ -54,6 +54,7 @@ struct LaunchCfg {
   int persistent = 0;
   int chunk = 1;
   int grid = 0;        // persistent grid (blocks)
+  int lean = 0;        // the lean form of the kernel (track_one)
   int eval32 = 0;      // the kernel carries the FP32 evaluation
   int plan_bytes = 0;  // table bytes the kernel stages into shared memory
   int ws_bytes = 0;
@@ -65,22 +66,27 @@ int device_smem_optin(int device);
 int device_sms(int device);
 // Tuned launch parameters remembered by phc_autotune for a device,
 // precision, schedule and register-row width; false if none.
-bool tuned_launch(int device, int precision, int schedule, int nm, int* warps, int* chunk);
-// Resolves the launch configuration for a plan on a device.
-int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, LaunchCfg* cfg);
+bool tuned_launch(int device, int precision, int schedule, int nm, int lean, int* warps,
+                  int* chunk);
+// Whether a launch of `paths` paths on a device uses the lean kernel form.
+bool use_lean(int64_t paths, int device);
+// Resolves the launch configuration for launches of about `paths` paths
+// of a plan on a device.
+int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, int64_t paths,
+                   LaunchCfg* cfg);
 // Launches the tracking kernel (phc_launch.cu).
 cudaError_t launch_track(const LaunchCfg& cfg, const KParams& kp, int grid, cudaStream_t s);
 // Occupancy (blocks per SM) of the kernel for a configuration.
 int track_blocks_per_sm(const LaunchCfg& cfg);
 // Batched kernel (many systems per launch) and its occupancy.
-cudaError_t launch_track_batch(int nm, int prec, int fac, int warps, int smem,
+cudaError_t launch_track_batch(int nm, int prec, int fac, int lean, int warps, int smem,
                                const KParamsBatch& kb, int grid, cudaStream_t s);
-int track_batch_blocks_per_sm(int nm, int prec, int fac, int warps, int smem);
-// Kernel variant: bit 0 the precision, mode / 2 the schedule form (1, 2, 3
-// factors per record).
-inline int kernel_mode(int prec, int fac) {
+int track_batch_blocks_per_sm(int nm, int prec, int fac, int lean, int warps, int smem);
+// Kernel variant: bit 0 the precision, (mode / 2) % 3 the schedule form (1,
+// 2, 3 factors per record), mode / 6 the lean form.
+inline int kernel_mode(int prec, int fac, int lean) {
   const int f = fac <= 1 ? 0 : (fac == 2 ? 1 : 2);
-  return (prec == PHC_PREC_MIXED ? 1 : 0) + 2 * f;
+  return (prec == PHC_PREC_MIXED ? 1 : 0) + 2 * f + (lean ? 6 : 0);
 }
 
 KOpts make_kopts(const phc_solve_options& so, const phc_gpu_options& g);

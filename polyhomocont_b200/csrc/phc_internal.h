@@ -81,8 +81,8 @@ struct alignas(16) PlanHeader {
   double gamma[2];
   double b[kMaxN][2];
   double patch[kMaxN][2];
-  // the patch row eliminated first (evaluate_rows_of; reduce = 1 for n = 8
-  // and n = 16): pivot column c, the largest |a_c| (first maximum),
+  // the patch row eliminated first (evaluate_rows_of; reduce = 1 for
+  // n = 16): pivot column c, the largest |a_c| (first maximum),
   // rho_j = a_j / a_c, 1/a_c, and the patch row's absolute sum sum_j |a_j|
   int32_t reduce;
   int32_t red_c;
@@ -230,21 +230,31 @@ inline int pick_nm(int rows) {
   return 0;
 }
 // The patch row is eliminated first where that moves the system into a
-// layout with more lanes per row: 9 and 17 unknowns have 8 and 16 equation
-// rows, which fit the four- and two-lane layouts (rows of up to 8 and 16).
-PHC_HD constexpr bool reduce_patch_row(int n) { return n == 8 || n == 16; }
+// layout with more lanes per row: 17 unknowns have 16 equation rows, which
+// fit the two-lane layout (rows of up to 16). (For 9 unknowns the same would
+// give the four-lane layout, but on one serving-stream system it turned a
+// path that the other form fails in 14,000 units into one that fails in the
+// end game after 3.2 million, so n = 8 keeps the patch as a row.)
+PHC_HD constexpr bool reduce_patch_row(int n) { return n == 16; }
 PHC_HD constexpr int eliminated_rows(int n) { return reduce_patch_row(n) ? n : n + 1; }
 // The single-system kernels of rows up to 8 columns carry an FP32
 // evaluation for the mixed predictor; every other kernel evaluates in FP64.
 PHC_HD constexpr bool kernel_eval32(int nm, int precision) {
   return precision == PHC_PREC_MIXED && nm <= 8;
 }
-// Most warps per block of the tracking kernels. Rows of up to 18 columns
-// are compiled for blocks of up to 12 warps, so that 12 warps share one
-// staged copy of the table; that bounds their registers at 65,536 / 384 =
-// 170 per thread, which they fit without spilling. The wider rows need more
-// registers and are compiled for blocks of up to 8 warps (255 registers).
-PHC_HD constexpr int max_warps_per_block(int nm) { return nm <= 18 ? 12 : 8; }
-constexpr int kMaxWarpsPerBlock = 12;  // over all row widths
+// Most warps per block of the tracking kernels. The lean form (the path
+// state out of registers across a unit, see track_one) of rows of up to 18
+// columns is compiled for blocks of up to 12 warps, so that 12 warps share
+// one staged copy of the table; that bounds its registers at 65,536 / 384 =
+// 170 per thread, which it fits without spilling. The other kernels are
+// compiled for blocks of up to 8 warps (255 registers).
+PHC_HD constexpr int max_warps_per_block(int nm, bool lean) {
+  return lean && nm <= 18 ? 12 : 8;
+}
+constexpr int kMaxWarpsPerBlock = 12;  // over all kernels
+// Resident warps per SM below which a launch is latency-bound: the form
+// that keeps the path state in registers is used for launches of at most
+// twice that many paths per SM, the lean form above.
+constexpr int kLeanPathsPerSm = 16;
 
 }  // namespace phc

@@ -24,7 +24,7 @@ PHC_DECLARE_NM(32)
 cudaError_t launch_track(const LaunchCfg& cfg, const KParams& kp, int grid, cudaStream_t s) {
   if (grid < 1) return cudaSuccess;
   const int block = cfg.warps * kWarp;
-  const int mode = kernel_mode(cfg.precision, cfg.fac);
+  const int mode = kernel_mode(cfg.precision, cfg.fac, cfg.lean);
   switch (cfg.nm) {
     case 6: return launch_nm_6(mode, kp, grid, block, cfg.smem, s);
     case 8: return launch_nm_8(mode, kp, grid, block, cfg.smem, s);
@@ -39,7 +39,7 @@ cudaError_t launch_track(const LaunchCfg& cfg, const KParams& kp, int grid, cuda
 
 int track_blocks_per_sm(const LaunchCfg& cfg) {
   const int block = cfg.warps * kWarp;
-  const int mode = kernel_mode(cfg.precision, cfg.fac);
+  const int mode = kernel_mode(cfg.precision, cfg.fac, cfg.lean);
   switch (cfg.nm) {
     case 6: return occupancy_nm_6(mode, block, cfg.smem);
     case 8: return occupancy_nm_8(mode, block, cfg.smem);
@@ -52,11 +52,11 @@ int track_blocks_per_sm(const LaunchCfg& cfg) {
   }
 }
 
-cudaError_t launch_track_batch(int nm, int prec, int fac, int warps, int smem,
+cudaError_t launch_track_batch(int nm, int prec, int fac, int lean, int warps, int smem,
                                const KParamsBatch& kb, int grid, cudaStream_t s) {
   if (grid < 1) return cudaSuccess;
   const int block = warps * kWarp;
-  const int mode = kernel_mode(prec, fac);
+  const int mode = kernel_mode(prec, fac, lean);
   switch (nm) {
     case 6: return launch_batch_nm_6(mode, kb, grid, block, smem, s);
     case 8: return launch_batch_nm_8(mode, kb, grid, block, smem, s);
@@ -69,9 +69,9 @@ cudaError_t launch_track_batch(int nm, int prec, int fac, int warps, int smem,
   }
 }
 
-int track_batch_blocks_per_sm(int nm, int prec, int fac, int warps, int smem) {
+int track_batch_blocks_per_sm(int nm, int prec, int fac, int lean, int warps, int smem) {
   const int block = warps * kWarp;
-  const int mode = kernel_mode(prec, fac);
+  const int mode = kernel_mode(prec, fac, lean);
   switch (nm) {
     case 6: return occupancy_batch_nm_6(mode, block, smem);
     case 8: return occupancy_batch_nm_8(mode, block, smem);

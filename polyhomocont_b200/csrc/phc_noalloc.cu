@@ -84,7 +84,7 @@ extern "C" int32_t phc_solve_paths_noalloc(const phc_system* sys, const phc_homo
   st = scratch_address(g.device, &scratch);
   if (st != PHC_OK) return st;
   LaunchCfg cfg;
-  st = resolve_launch(hp, g, g.device, &cfg);
+  st = resolve_launch(hp, g, g.device, count, &cfg);
   if (st != PHC_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the counter must start at zero; the table is rewritten by every call.

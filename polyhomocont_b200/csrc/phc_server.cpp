@@ -201,9 +201,11 @@ int launch_batch(phc_server* S, Slot& s) {
     ws_cap = std::max(ws_cap, ws_layout(r.plan.n, r.plan.S, r.plan.pw_size, false).bytes);
   }
   const int slice = table_cap + ws_cap + align16((int)sizeof(KOpts));
+  // the lean kernel form for batches with many more paths than resident warps
+  const int lean = use_lean(total, S->cfg.device) ? 1 : 0;
   const int smax = device_smem_optin(S->cfg.device);
   int warps = g.warps_per_block > 0
-                  ? std::min(std::max(g.warps_per_block, 1), max_warps_per_block(nm))
+                  ? std::min(std::max(g.warps_per_block, 1), max_warps_per_block(nm, lean != 0))
                   : 4;
   while (warps > 1 && warps * slice > smax) --warps;
   if (warps * slice > smax) {
@@ -211,7 +213,7 @@ int launch_batch(phc_server* S, Slot& s) {
     return PHC_ERR_UNSUPPORTED;
   }
   const int smem = warps * slice;
-  int bps = track_batch_blocks_per_sm(nm, prec, fac, warps, smem);
+  int bps = track_batch_blocks_per_sm(nm, prec, fac, lean, warps, smem);
   if (bps < 1) bps = 1;
   if (g.blocks_per_sm > 0) bps = std::min(bps, g.blocks_per_sm);
   KParamsBatch kb;
@@ -236,7 +238,7 @@ int launch_batch(phc_server* S, Slot& s) {
   if (e != cudaSuccess) return cuda_fail(e, "server H2D");
   e = cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long), s.stream);
   if (e != cudaSuccess) return cuda_fail(e, "server counter reset");
-  e = launch_track_batch(nm, prec, fac, warps, smem, kb, grid, s.stream);
+  e = launch_track_batch(nm, prec, fac, lean, warps, smem, kb, grid, s.stream);
   if (e != cudaSuccess) return cuda_fail(e, "server kernel launch");
   // each request's results are copied back as soon as its paths are done
   // (see engine_main); the event marks the end of the whole batch
@@ -514,7 +516,7 @@ int32_t phc_server_submit(phc_server* S, const phc_system* sys, const phc_solve_
   st = build_plan(&v, &hv, &r->plan);
   if (st != PHC_OK) return st;
   r->npaths = r->hom.nstart;
-  st = resolve_launch(r->plan, S->cfg.gpu, S->cfg.device, &r->cfg);
+  st = resolve_launch(r->plan, S->cfg.gpu, S->cfg.device, r->npaths, &r->cfg);
   if (st != PHC_OK) return st;
   r->dev_bytes = sizeof(BatchSys) + up256(r->plan.bytes.size()) + up256((size_t)r->npaths * sizeof(phc_path_out)) +
                  up256((size_t)r->npaths * (r->n + 1) * 16) + up256((size_t)r->npaths * r->n * 16);

@@ -141,22 +141,18 @@ __device__ __forceinline__ cd full_solution(const PlanHeader& P, const WarpConst
   return (lane == c) ? xc : x;
 }
 
-// The unit reads the system's constants and its workspace pointers from
-// shared memory itself (tbl: the staged table, wbase: the warp's
-// workspace), so that nothing of them stays live in registers between
-// units. With the patch row eliminated first (the header's `reduce`) it
-// works on the n x n reduced system and returns the solution of the full
-// one.
+// One unit on the staged table tbl with the system's constants C and the
+// warp's workspace ws. With the patch row eliminated first (the header's
+// `reduce`) it works on the n x n reduced system and returns the solution
+// of the full one.
 template <int NM, bool MIXED, bool EVAL32, int F>
-__device__ __forceinline__ void run_unit(const unsigned char* tbl, unsigned char* wbase, int kind,
-                                         int prec, int c0, cd zin, cd t, cd dt, int lane,
-                                         UnitRes& u) {
+__device__ __forceinline__ void run_unit(const unsigned char* tbl, const WarpConst& C,
+                                         const WarpWS& ws, int kind, int prec, int c0, cd zin,
+                                         cd t, cd dt, int lane, UnitRes& u) {
   using L = RowLayout<NM>;
   constexpr int RW = L::kRegs;
   constexpr int S = L::kLanes;
   const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(tbl);
-  const WarpConst C = load_warp_const(P, tbl, lane);
-  const WarpWS ws = warp_workspace<EVAL32>(P, wbase);
   const int n = C.n, N = C.N, c = C.red_c;
   const bool reduce = P.reduce != 0;
   const int rows = reduce ? n : N;  // rows of the eliminated system
@@ -401,30 +397,47 @@ __device__ __forceinline__ double vnorm2(cd v, int lane, int N) {
 
 // Tracks path k (1-based) and writes its record, z and x.
 //
-// The state of the path -- the lane vectors z, the segment's start point
-// zs, the prediction zp and the RK4 sum, the segment stepper's scalars, the
-// pending unit's inputs -- lives in the warp's WarpState in shared memory,
-// not in registers: the state machine touches it a few times per unit,
-// while the unit (an evaluation and an elimination, thousands of
-// instructions) then has the register file to itself. Only the control
-// state pc and the unit's result U stay in registers across a unit.
-template <int NM, int PREC, bool EVAL32, int F>
+// The hot state of the path (z, the segment's start point zs, the corrector's
+// point zp, the RK4 sum, the segment stepper's scalars) lives in registers
+// while the state machine runs. LEAN selects what happens across a unit:
+//   LEAN = false: the state and the system's constants (WarpConst, the
+//     workspace pointers, loaded once) stay in registers. Fewest
+//     instructions and dependent shared-memory round trips per unit: the
+//     form for launches in which one path's latency sets the time.
+//   LEAN = true: the state is stored to the warp's WarpState before the unit
+//     and loaded back after it (independent stores and loads, issued
+//     together), and the unit loads the constants itself, so that neither
+//     occupies registers while the unit runs. About 70 registers fewer per
+//     thread (134 against 210 for 16-column rows), hence more resident warps:
+//     the form for launches with many more paths than resident warps.
+template <int NM, int PREC, bool EVAL32, int F, bool LEAN>
 __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned char* wbase,
                                           WarpState& st, const KOpts& O, int64_t k, int lane,
                                           phc_path_out* rec, double* zo, double* xo) {
   const phc_tracker_options& TO = O.so.tracker;
   const phc_endgame_options& EO = O.so.endgame;
+  const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(tbl);
+  // the constants the unit reads, held for the whole path (not LEAN)
+  const WarpConst C0 = load_warp_const(P, tbl, lane);
+  const WarpWS ws0 = warp_workspace<EVAL32>(P, wbase);
   constexpr bool kMixed = (PREC == PHC_PREC_MIXED);
+
+  // hot lane vectors (component j in lane j)
+  cd z = czero<double>(), zs = z, zp = z, ksum = z, zin = z;
+  // hot uniform state of the segment being tracked
+  double s = 0.0, step = 0.0, ds = 0.0, sn = 0.0, dnorm_prev = kHuge;
+  int nsucc = 0, sacc = 0, srej = 0, sstat = PHC_PATH_SUCCESS, stage = 0;
+  bool att64 = true;
+  // pending unit
+  int uk = UK_TANGENT, pc_after = PC_FINISH;
+  int u_prec = 0;  // 0: FP64, 1: FP64 evaluation + FP32 elimination, 2: FP32 evaluation + elimination
+  cd tin = z, dtin = z;
   UnitRes U;
   U.x = U.h = czero<double>();
   U.a1 = U.a2 = 0.0;
   U.ok = true;
 
   // path result defaults (type(path_result), src/solve.f90:86-119)
-  st.kpath = k;
-  st.rec = rec;
-  st.zo = zo;
-  st.xo = xo;
   st.p_status = PHC_PATH_SUCCESS;
   st.p_wind = st.p_egs = st.p_nacc = st.p_nrej = 0;
   st.p_t = 1.0;
@@ -434,23 +447,23 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
   st.units = 0;
   st.sticky = 0;
   st.cond_c0 = 0;
-  st.dnorm_prev = kHuge;
+  st.kpath = k;
+  st.rec = rec;
+  st.zo = zo;
+  st.xo = xo;
   STV(xv, czero<double>());
 
   int pc = PC_START;
   for (;;) {
     bool want = false;
+    const int n = P.n, N = P.N;
     while (!want) {
-      const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(tbl);
-      const int n = P.n, N = P.N;
       switch (pc) {
         case PC_START: {
           // tdh_start_solution, src/homotopy.f90:151-177
-          const int64_t kk = st.kpath;
-          cd z = czero<double>();
           if (lane < n) {
             const int d = P.deg[lane];
-            const int64_t digit = ((kk - 1) / P.radix[lane]) % d;
+            const int64_t digit = ((st.kpath - 1) / P.radix[lane]) % d;
             const double phi = (P.argb[lane] + 2.0 * kPi * (double)digit) / (double)d;
             double sp, cp;
             sincos(phi, &sp, &cp);
@@ -462,7 +475,6 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
                                    : czero<double>();
           const cd sum = warp_csum(pz);
           if (lane < N) z = cdiv(z, sum);
-          STV(z, z);
           // track_path(hom, z, 1, t_end), src/solve.f90:230-232
           st.seg_arc = 0;
           st.seg_t0[0] = 1.0;
@@ -472,7 +484,7 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           st.o_step_init = TO.step_init;
           st.o_step_max = TO.step_max;
           st.o_grow = TO.grow_after;
-          STV(zs, z);
+          zs = z;
           st.seg_cont = PC_MAIN_DONE;
           pc = PC_SEG_BEGIN;
           break;
@@ -480,98 +492,86 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
 
         // ---------------- track_segment, src/tracker.f90:196-264 -------------
         case PC_SEG_BEGIN:
-          st.s = 0.0;
-          st.step = fmin(st.o_step_init, st.o_step_max);
-          st.nsucc = 0;
-          st.sacc = 0;
-          st.srej = 0;
-          st.sstat = PHC_PATH_SUCCESS;
+          s = 0.0;
+          step = fmin(st.o_step_init, st.o_step_max);
+          nsucc = 0;
+          sacc = 0;
+          srej = 0;
+          sstat = PHC_PATH_SUCCESS;
           pc = PC_SEG_ATTEMPT;
           break;
 
         case PC_SEG_ATTEMPT: {
-          const double s = st.s, step = st.step;
           if (!(s < 1.0)) {
             pc = PC_SEG_END;
             break;
           }
-          if (st.sacc + st.srej >= TO.max_steps || st.units > O.max_units) {
-            st.sstat = PHC_PATH_FAILED_MAX_STEPS;
+          if (sacc + srej >= TO.max_steps || st.units > O.max_units) {
+            sstat = PHC_PATH_FAILED_MAX_STEPS;
             pc = PC_SEG_END;
             break;
           }
-          double ds = fmin(step, 1.0 - s);
-          double sn = s + ds;
+          ds = fmin(step, 1.0 - s);
+          sn = s + ds;
           if (1.0 - sn <= 1.0e-3 * step) {
             sn = 1.0;
             ds = 1.0 - s;
           }
-          st.ds = ds;
-          st.sn = sn;
           const int sticky = st.sticky;
-          const bool att64 = !kMixed || sticky > 0;
-          st.att64 = att64 ? 1 : 0;
+          att64 = !kMixed || sticky > 0;
           if (sticky > 0) st.sticky = sticky - 1;
           // predict_rk4 stage 1: tangent at (z, s), src/tracker.f90:283
-          st.stage = 0;
-          st.uk = UK_TANGENT;
-          st.u_prec = att64 ? 0 : (EVAL32 ? 2 : 1);
-          STV(zin, LDV(zs));
-          seg_tdt_store(st, s);
-          st.pc_after = PC_SEG_AFTER_UNIT;
+          stage = 0;
+          uk = UK_TANGENT;
+          u_prec = att64 ? 0 : (EVAL32 ? 2 : 1);
+          zin = zs;
+          seg_tdt(st, s, tin, dtin);
+          pc_after = PC_SEG_AFTER_UNIT;
           want = true;
           break;
         }
 
         case PC_SEG_AFTER_UNIT: {
           int outcome = 0;  // 1 accept, 2 reject
-          const int stage = st.stage;
           if (stage < 4) {
             ++st.c_tan;
             if (!U.ok) {
               outcome = 2;
             } else {
               // predict_rk4, src/tracker.f90:266-293
-              const double s = st.s, ds = st.ds;
               const cd kk = U.x;
-              const cd zs = LDV(zs);
               double s_in = s;
               if (stage == 0) {
-                STV(ksum, kk);
-                STV(zin, zs + (0.5 * ds) * kk);
+                ksum = kk;
+                zin = zs + (0.5 * ds) * kk;
                 s_in = s + 0.5 * ds;
               } else if (stage == 1) {
-                STV(ksum, LDV(ksum) + 2.0 * kk);
-                STV(zin, zs + (0.5 * ds) * kk);
+                ksum = ksum + 2.0 * kk;
+                zin = zs + (0.5 * ds) * kk;
                 s_in = s + 0.5 * ds;
               } else if (stage == 2) {
-                STV(ksum, LDV(ksum) + 2.0 * kk);
-                STV(zin, zs + ds * kk);
+                ksum = ksum + 2.0 * kk;
+                zin = zs + ds * kk;
                 s_in = s + ds;
               } else {
-                const cd ksum = LDV(ksum) + kk;
-                STV(zp, zs + (ds / 6.0) * ksum);
+                ksum = ksum + kk;
+                zp = zs + (ds / 6.0) * ksum;
               }
               if (stage < 3) {
-                st.stage = stage + 1;
-                st.uk = UK_TANGENT;
+                ++stage;
+                uk = UK_TANGENT;
                 // stages 1 and 2 share s + ds/2: t and dt/ds are reused
-                if (stage + 1 != 2) seg_tdt_store(st, s_in);
+                if (stage != 2) seg_tdt(st, s_in, tin, dtin);
               } else {
                 // newton_correct at t(sn), src/tracker.f90:319-360
-                st.stage = 4;
-                st.dnorm_prev = kHuge;
-                st.uk = UK_NEWTON;
-                st.u_prec = st.att64 ? 0 : 1;
-                STV(zin, LDV(zp));
-                const double sn = st.sn;
-                if (sn != s + ds) {  // else t(s + ds) of stage 3
-                  const cd t = seg_t(st, sn);
-                  st.tin[0] = t.re;
-                  st.tin[1] = t.im;
-                }
+                stage = 4;
+                dnorm_prev = kHuge;
+                uk = UK_NEWTON;
+                u_prec = att64 ? 0 : 1;
+                zin = zp;
+                if (sn != s + ds) tin = seg_t(st, sn);  // else t(s + ds) of stage 3
               }
-              st.pc_after = PC_SEG_AFTER_UNIT;
+              pc_after = PC_SEG_AFTER_UNIT;
               want = true;
               break;
             }
@@ -581,24 +581,23 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
             if (!U.ok) {
               outcome = 2;
             } else {
-              const cd zp = LDV(zp) + U.x;
-              STV(zp, zp);
+              zp = zp + U.x;
               // ||dz|| <= tol ||z|| and the contraction test on squared norms
               const double d2 = vnorm2(U.x, lane, N);
               const double z2 = vnorm2(zp, lane, N);
               if (d2 <= (TO.corrector_tol * TO.corrector_tol) * z2) {
                 outcome = 1;
-              } else if (it > 1 && d2 > (TO.contraction * TO.contraction) * st.dnorm_prev) {
+              } else if (it > 1 && d2 > (TO.contraction * TO.contraction) * dnorm_prev) {
                 outcome = 2;
               } else {
-                st.dnorm_prev = d2;
+                dnorm_prev = d2;
                 if (it >= TO.corrector_maxit) {
                   outcome = 2;
                 } else {
-                  st.stage = stage + 1;
-                  st.uk = UK_NEWTON;
-                  STV(zin, zp);
-                  st.pc_after = PC_SEG_AFTER_UNIT;
+                  ++stage;
+                  uk = UK_NEWTON;
+                  zin = zp;
+                  pc_after = PC_SEG_AFTER_UNIT;
                   want = true;
                   break;
                 }
@@ -606,38 +605,35 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
             }
           }
           if (outcome == 1) {
-            STV(zs, LDV(zp));
-            st.s = st.sn;
-            ++st.sacc;
-            const int nsucc = st.nsucc + 1;
+            zs = zp;
+            s = sn;
+            ++sacc;
+            ++nsucc;
             if (nsucc >= st.o_grow) {
-              st.step = fmin(2.0 * st.step, st.o_step_max);
-              st.nsucc = 0;
-            } else {
-              st.nsucc = nsucc;
+              step = fmin(2.0 * step, st.o_step_max);
+              nsucc = 0;
             }
             pc = PC_SEG_ATTEMPT;
           } else {
-            if (kMixed && !st.att64) {
+            if (kMixed && !att64) {
               // the FP32 attempt failed: redo the same step in FP64 before
               // counting a rejection, and stay in FP64 for a few steps
-              st.att64 = 1;
+              att64 = true;
               st.sticky = O.fp64_sticky;
-              st.stage = 0;
-              st.uk = UK_TANGENT;
-              st.u_prec = 0;
-              STV(zin, LDV(zs));
-              seg_tdt_store(st, st.s);
-              st.pc_after = PC_SEG_AFTER_UNIT;
+              stage = 0;
+              uk = UK_TANGENT;
+              u_prec = 0;
+              zin = zs;
+              seg_tdt(st, s, tin, dtin);
+              pc_after = PC_SEG_AFTER_UNIT;
               want = true;
               break;
             }
-            ++st.srej;
-            st.nsucc = 0;
-            const double step = 0.5 * st.step;
-            st.step = step;
+            ++srej;
+            nsucc = 0;
+            step = 0.5 * step;
             if (step < TO.step_min) {
-              st.sstat = PHC_PATH_FAILED_MIN_STEP;
+              sstat = PHC_PATH_FAILED_MIN_STEP;
               pc = PC_SEG_END;
             } else {
               pc = PC_SEG_ATTEMPT;
@@ -651,13 +647,12 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           break;
 
         // ---------------- endpoint, src/solve.f90:217-252 ----------------------
-        case PC_MAIN_DONE: {
-          STV(z, LDV(zs));
-          const int sstat = st.sstat;
+        case PC_MAIN_DONE:
+          z = zs;
           st.p_status = sstat;
-          st.p_t = seg_t(st, st.s).re;
-          st.p_nacc = st.sacc;
-          st.p_nrej = st.srej;
+          st.p_t = seg_t(st, s).re;
+          st.p_nacc = sacc;
+          st.p_nrej = srej;
           if (sstat != PHC_PATH_SUCCESS)
             pc = PC_FINISH;
           else if (!O.so.use_endgame)
@@ -665,13 +660,12 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           else
             pc = PC_EG_INIT;
           break;
-        }
 
         // ---------------- cauchy_endgame, src/endgame.f90:124-267 --------------
         case PC_EG_INIT:
           st.eg_segstep = 1.0;  // segopts: step_init = step_max = 1, grow_after = 2
           st.eg_status = PHC_ENDGAME_FAILED;
-          STV(resz, LDV(z));
+          STV(resz, z);
           st.r = EO.t_start;
           st.have_prev = 0;
           st.best_resid = kHuge;
@@ -729,9 +723,8 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
             pc = PC_EG_DONE;
             break;
           }
-          const cd z = LDV(z);
           STV(zold, z);
-          STV(zs, z);
+          zs = z;
           st.seg_arc = 0;
           st.seg_t0[0] = st.r;
           st.seg_t0[1] = 0.0;
@@ -746,13 +739,13 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
         }
 
         case PC_EG_AFTER_RADIAL: {
-          cd z = LDV(zs);
-          st.eg_segstep = fmin(fmax(st.step, TO.step_min), 1.0);
-          st.eg_nacc += st.sacc;
-          st.eg_nrej += st.srej;
+          z = zs;
+          st.eg_segstep = fmin(fmax(step, TO.step_min), 1.0);
+          st.eg_nacc += sacc;
+          st.eg_nrej += srej;
           const cd zold = LDV(zold);
-          if (st.sstat != PHC_PATH_SUCCESS) {
-            STV(z, zold);
+          if (sstat != PHC_PATH_SUCCESS) {
+            z = zold;
             if (!(st.gate || st.r < EO.loop_radius)) {
               st.lp_max = EO.max_winding;
               st.lp_cont = PC_EG_AFTER_FALLBACK;
@@ -762,7 +755,6 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
             }
             break;
           }
-          STV(z, z);
           st.r = st.rnew;
           // winding number estimate from the radial differences
           const double d = vnorm(z - zold, lane, N);
@@ -795,11 +787,10 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           }
           break;
 
-        case PC_LOOPS_BEGIN: {
-          const cd z = LDV(z);
+        case PC_LOOPS_BEGIN:
           st.lp_dth = 2.0 * kPi / (double)EO.nsamples;
           st.lp_floor = 10.0 * TO.corrector_tol * vnorm(z, lane, N);
-          STV(zs, z);
+          zs = z;
           STV(zsum, czero<double>());
           st.lp_nsamp = 0;
           st.lp_spacing = kHuge;
@@ -807,10 +798,8 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           st.lp_j = 1;
           pc = PC_LOOP_ARC;
           break;
-        }
 
-        case PC_LOOP_ARC: {
-          const cd zs = LDV(zs);
+        case PC_LOOP_ARC:
           STV(zsum, LDV(zsum) + zs);
           ++st.lp_nsamp;
           STV(zprev, zs);
@@ -824,18 +813,16 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           st.seg_cont = PC_LOOP_AFTER_ARC;
           pc = PC_SEG_BEGIN;
           break;
-        }
 
         case PC_LOOP_AFTER_ARC: {
-          st.eg_segstep = fmin(fmax(st.step, TO.step_min), 1.0);
-          st.eg_nacc += st.sacc;
-          st.eg_nrej += st.srej;
-          if (st.sstat != PHC_PATH_SUCCESS) {
+          st.eg_segstep = fmin(fmax(step, TO.step_min), 1.0);
+          st.eg_nacc += sacc;
+          st.eg_nrej += srej;
+          if (sstat != PHC_PATH_SUCCESS) {
             st.lp_ok = 0;
             pc = st.lp_cont;
             break;
           }
-          const cd zs = LDV(zs);
           st.lp_spacing = fmin(st.lp_spacing, vnorm(zs - LDV(zprev), lane, N));
           const int j = st.lp_j + 1;
           st.lp_j = j;
@@ -843,8 +830,7 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
             pc = PC_LOOP_ARC;
             break;
           }
-          if (vnorm(zs - LDV(z), lane, N) <=
-              fmax(EO.closure_factor * st.lp_spacing, st.lp_floor)) {
+          if (vnorm(zs - z, lane, N) <= fmax(EO.closure_factor * st.lp_spacing, st.lp_floor)) {
             const double inv = (double)st.lp_nsamp;
             const cd zsum = LDV(zsum);
             STV(est, mkc<double>(zsum.re / inv, zsum.im / inv));
@@ -871,12 +857,12 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           if (st.have_prev)
             err = vnorm(est - LDV(prev), lane, N) / fmax(vnorm(est, lane, N), kTiny);
           st.rec_err = err;
-          st.uk = UK_BACKERR;
-          st.u_prec = 0;
-          STV(zin, est);
-          st.tin[0] = st.tin[1] = 0.0;
-          st.dtin[0] = st.dtin[1] = 0.0;
-          st.pc_after = PC_RECORD_AFTER;
+          uk = UK_BACKERR;
+          u_prec = 0;
+          zin = est;
+          tin = czero<double>();
+          dtin = czero<double>();
+          pc_after = PC_RECORD_AFTER;
           want = true;
           break;
         }
@@ -884,7 +870,6 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
         case PC_RECORD_AFTER: {
           ++st.c_eval;
           const double err = st.rec_err;
-          const cd zin = LDV(zin);
           const double resid = U.a1 / fmax(U.a2 * vnorm(zin, lane, N), kTiny);
           if (st.eg_status == PHC_ENDGAME_FAILED ||
               better(resid, err, st.best_resid, st.eg_error, EO.residual_tol)) {
@@ -908,7 +893,7 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
             st.p_status = PHC_PATH_ENDGAME_FAILED;
             pc = PC_FINISH;
           } else {
-            STV(z, LDV(resz));
+            z = LDV(resz);
             st.p_t = 0.0;
             st.p_wind = st.eg_wind;
             st.p_egs = st.eg_status;
@@ -919,14 +904,14 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
 
         // ---------------- classify, src/solve.f90:288-328 ---------------------
         case PC_CL_START:
-          st.uk = UK_COND;
-          st.u_prec = 0;
-          STV(zin, LDV(z));
-          st.tin[0] = st.tin[1] = 0.0;
-          st.dtin[0] = st.dtin[1] = 0.0;
+          uk = UK_COND;
+          u_prec = 0;
+          zin = z;
+          tin = czero<double>();
+          dtin = czero<double>();
           st.cond_c0 = 0;
           st.cond_ret = PC_CL_AFTER_COND1;
-          st.pc_after = PC_COND_STEP;
+          pc_after = PC_COND_STEP;
           want = true;
           break;
 
@@ -944,8 +929,8 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           st.cond_ainv = ainv;
           if (c0 + kCondChunk < N) {
             st.cond_c0 = c0 + kCondChunk;
-            st.uk = UK_COND;
-            st.pc_after = PC_COND_STEP;
+            uk = UK_COND;
+            pc_after = PC_COND_STEP;
             want = true;
             break;
           }
@@ -965,10 +950,10 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           if (!sing && O.so.refine_maxit >= 1) {
             // refine, src/solve.f90:254-286
             st.rf_it = 1;
-            st.dnorm_prev = kHuge;
-            st.uk = UK_REFINE;
-            STV(zin, LDV(z));
-            st.pc_after = PC_CL_AFTER_REFINE;
+            dnorm_prev = kHuge;
+            uk = UK_REFINE;
+            zin = z;
+            pc_after = PC_CL_AFTER_REFINE;
             want = true;
           } else {
             pc = sing ? PC_CL_FINAL : PC_CL_COND2;
@@ -983,37 +968,36 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
             break;
           }
           const double dnorm = vnorm(U.x, lane, N);
-          if (dnorm > st.dnorm_prev) {
+          if (dnorm > dnorm_prev) {
             pc = PC_CL_COND2;
             break;
           }
-          const cd z = LDV(z) + U.x;
-          STV(z, z);
+          z = z + U.x;
           if (dnorm <= 4.0 * kEps * vnorm(z, lane, N)) {
             pc = PC_CL_COND2;
             break;
           }
-          st.dnorm_prev = dnorm;
+          dnorm_prev = dnorm;
           const int it = st.rf_it + 1;
           st.rf_it = it;
           if (it > O.so.refine_maxit) {
             pc = PC_CL_COND2;
             break;
           }
-          st.uk = UK_REFINE;
-          STV(zin, z);
-          st.pc_after = PC_CL_AFTER_REFINE;
+          uk = UK_REFINE;
+          zin = z;
+          pc_after = PC_CL_AFTER_REFINE;
           want = true;
           break;
         }
 
         case PC_CL_COND2:
-          st.uk = UK_COND;
-          st.u_prec = 0;
-          STV(zin, LDV(z));
+          uk = UK_COND;
+          u_prec = 0;
+          zin = z;
           st.cond_c0 = 0;
           st.cond_ret = PC_CL_AFTER_COND2;
-          st.pc_after = PC_COND_STEP;
+          pc_after = PC_COND_STEP;
           want = true;
           break;
 
@@ -1026,7 +1010,6 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           break;
 
         case PC_CL_FINAL: {
-          const cd z = LDV(z);
           const double znorm = vnorm(z, lane, N);
           const double ri =
               (lane < n) ? cabs(LDV(hsave)) / rpowi(znorm, P.deg[lane]) : 0.0;
@@ -1076,7 +1059,6 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
           double* zo_ = st.zo;
           double* xo_ = st.xo;
           if (lane < N) {
-            const cd z = LDV(z);
             zo_[2 * lane] = z.re;
             zo_[2 * lane + 1] = z.im;
           }
@@ -1091,18 +1073,63 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
       }
     }
     // ---- run the requested unit ----
-    {
-      const int uk = st.uk;
-      const int u_prec = kMixed ? st.u_prec : 0;
-      const cd zin = LDV(zin);
-      const cd tin = mkc<double>(st.tin[0], st.tin[1]);
-      const cd dtin = mkc<double>(st.dtin[0], st.dtin[1]);
-      run_unit<NM, kMixed, EVAL32, F>(tbl, wbase, uk, u_prec, st.cond_c0, zin, tin, dtin, lane,
-                                      U);
-      if (kMixed && u_prec == 0 && uk <= UK_NEWTON) ++st.c_retry;  // predictor/corrector unit in FP64
-      ++st.units;
+    if constexpr (LEAN) {
+      // the path's state goes to the warp state for the unit's duration
+      STV(z, z);
+      STV(zs, zs);
+      STV(zp, zp);
+      STV(ksum, ksum);
+      st.s = s;
+      st.step = step;
+      st.ds = ds;
+      st.sn = sn;
+      st.dnorm_prev = dnorm_prev;
+      st.tin[0] = tin.re;
+      st.tin[1] = tin.im;
+      st.dtin[0] = dtin.re;
+      st.dtin[1] = dtin.im;
+      st.nsucc = nsucc;
+      st.sacc = sacc;
+      st.srej = srej;
+      st.sstat = sstat;
+      st.stage = stage;
+      st.att64 = att64 ? 1 : 0;
+      st.uk = uk;
+      st.pc_after = pc_after;
+      st.u_prec = u_prec;
+      {
+        const WarpConst C = load_warp_const(P, tbl, lane);
+        const WarpWS ws = warp_workspace<EVAL32>(P, wbase);
+        run_unit<NM, kMixed, EVAL32, F>(tbl, C, ws, uk, kMixed ? u_prec : 0, st.cond_c0, zin,
+                                        tin, dtin, lane, U);
+      }
+      z = LDV(z);
+      zs = LDV(zs);
+      zp = LDV(zp);
+      ksum = LDV(ksum);
+      s = st.s;
+      step = st.step;
+      ds = st.ds;
+      sn = st.sn;
+      dnorm_prev = st.dnorm_prev;
+      tin = mkc<double>(st.tin[0], st.tin[1]);
+      dtin = mkc<double>(st.dtin[0], st.dtin[1]);
+      nsucc = st.nsucc;
+      sacc = st.sacc;
+      srej = st.srej;
+      sstat = st.sstat;
+      stage = st.stage;
+      att64 = st.att64 != 0;
+      uk = st.uk;
+      u_prec = st.u_prec;
+      pc_after = st.pc_after;
+    } else {
+      run_unit<NM, kMixed, EVAL32, F>(tbl, C0, ws0, uk, kMixed ? u_prec : 0, st.cond_c0, zin,
+                                      tin, dtin, lane, U);
     }
-    pc = st.pc_after;
+    if (kMixed && u_prec == 0 && uk <= UK_NEWTON) ++st.c_retry;  // predictor/corrector unit in FP64
+    ++st.units;
+    pc = pc_after;
   }
 }
 
@@ -1127,13 +1154,13 @@ __device__ __forceinline__ void init_jacobian_buffer(const PlanHeader& P, unsign
   __syncwarp();
 }
 
-// Threads per block the kernels of a row width are compiled for.
-template <int NM>
-constexpr int kMaxBlockThreads = max_warps_per_block(NM) * kWarp;
+// Threads per block the kernels of a row width and form are compiled for.
+template <int NM, bool LEAN>
+constexpr int kMaxBlockThreads = max_warps_per_block(NM, LEAN) * kWarp;
 
 // Single-system kernel: every block stages the table once for its warps.
-template <int NM, int PREC, int F>
-__global__ void __launch_bounds__(kMaxBlockThreads<NM>) track_kernel(const KParams kp) {
+template <int NM, int PREC, int F, bool LEAN>
+__global__ void __launch_bounds__(kMaxBlockThreads<NM, LEAN>) track_kernel(const KParams kp) {
   extern __shared__ __align__(16) unsigned char smem[];
   // the single-system kernels of narrow rows carry the FP32 evaluation
   constexpr bool E32 = kernel_eval32(NM, PREC);
@@ -1170,8 +1197,8 @@ __global__ void __launch_bounds__(kMaxBlockThreads<NM>) track_kernel(const KPara
       if (q >= kp.count) break;
     }
     const int n = P.n, N = P.N;
-    track_one<NM, PREC, E32, F>(smem, wbase, *stp, kp.opts, kp.k0 + q, lane, kp.out + q,
-                                kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
+    track_one<NM, PREC, E32, F, LEAN>(smem, wbase, *stp, kp.opts, kp.k0 + q, lane, kp.out + q,
+                                      kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
   }
 }
 
@@ -1179,8 +1206,8 @@ __global__ void __launch_bounds__(kMaxBlockThreads<NM>) track_kernel(const KPara
 // options) in one launch. Persistent warps pull global path indices from
 // one queue; a warp that moves on to another system stages that system's
 // table and options into its own shared-memory slice.
-template <int NM, int PREC, int F>
-__global__ void __launch_bounds__(kMaxBlockThreads<NM>)
+template <int NM, int PREC, int F, bool LEAN>
+__global__ void __launch_bounds__(kMaxBlockThreads<NM, LEAN>)
     track_batch_kernel(const KParamsBatch kb) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1231,7 +1258,7 @@ __global__ void __launch_bounds__(kMaxBlockThreads<NM>)
     phc_path_out* out = reinterpret_cast<phc_path_out*>(kb.base + S.out_off) + kl;
     double* z = reinterpret_cast<double*>(kb.base + S.z_off) + 2 * kl * N;
     double* x = S.x_off >= 0 ? reinterpret_cast<double*>(kb.base + S.x_off) + 2 * kl * n : nullptr;
-    track_one<NM, PREC, false, F>(tbl, wbase, *stp, *opts, kl + 1, lane, out, z, x);
+    track_one<NM, PREC, false, F, LEAN>(tbl, wbase, *stp, *opts, kl + 1, lane, out, z, x);
     if (kb.done != nullptr) {
       // every lane's result stores are made visible system-wide before the
       // path is counted as finished
@@ -1246,25 +1273,32 @@ __global__ void __launch_bounds__(kMaxBlockThreads<NM>)
 
 // Host-side launch and occupancy helpers of one register-row width NM,
 // defined in the instantiation units track_nm*.cu.
-// mode: bit 0 the precision (PHC_PREC_*), mode / 2 + 1 the schedule form
+// mode: bit 0 the precision (PHC_PREC_*), (mode / 2) % 3 + 1 the schedule
+// form, mode / 6 the lean form (kernel_mode in phc_host.h)
 #define PHC_FOR_MODES(MACRO, NMV, ...)                                            \
   switch (mode) {                                                                 \
-    case 0: MACRO(NMV, PHC_PREC_FP64, 1, __VA_ARGS__); break;                     \
-    case 1: MACRO(NMV, PHC_PREC_MIXED, 1, __VA_ARGS__); break;                    \
-    case 2: MACRO(NMV, PHC_PREC_FP64, 2, __VA_ARGS__); break;                     \
-    case 3: MACRO(NMV, PHC_PREC_MIXED, 2, __VA_ARGS__); break;                    \
-    case 4: MACRO(NMV, PHC_PREC_FP64, 3, __VA_ARGS__); break;                     \
-    default: MACRO(NMV, PHC_PREC_MIXED, 3, __VA_ARGS__); break;                   \
+    case 0: MACRO(NMV, PHC_PREC_FP64, 1, false, __VA_ARGS__); break;              \
+    case 1: MACRO(NMV, PHC_PREC_MIXED, 1, false, __VA_ARGS__); break;             \
+    case 2: MACRO(NMV, PHC_PREC_FP64, 2, false, __VA_ARGS__); break;              \
+    case 3: MACRO(NMV, PHC_PREC_MIXED, 2, false, __VA_ARGS__); break;             \
+    case 4: MACRO(NMV, PHC_PREC_FP64, 3, false, __VA_ARGS__); break;              \
+    case 5: MACRO(NMV, PHC_PREC_MIXED, 3, false, __VA_ARGS__); break;             \
+    case 6: MACRO(NMV, PHC_PREC_FP64, 1, true, __VA_ARGS__); break;               \
+    case 7: MACRO(NMV, PHC_PREC_MIXED, 1, true, __VA_ARGS__); break;              \
+    case 8: MACRO(NMV, PHC_PREC_FP64, 2, true, __VA_ARGS__); break;               \
+    case 9: MACRO(NMV, PHC_PREC_MIXED, 2, true, __VA_ARGS__); break;              \
+    case 10: MACRO(NMV, PHC_PREC_FP64, 3, true, __VA_ARGS__); break;              \
+    default: MACRO(NMV, PHC_PREC_MIXED, 3, true, __VA_ARGS__); break;             \
   }
-#define PHC_SET_ATTR(NMV, PR, FF, smax)                                            \
-  cudaFuncSetAttribute(track_kernel<NMV, PR, FF>,                                 \
+#define PHC_SET_ATTR(NMV, PR, FF, LN, smax)                                        \
+  cudaFuncSetAttribute(track_kernel<NMV, PR, FF, LN>,                             \
                        cudaFuncAttributeMaxDynamicSharedMemorySize, smax);        \
-  cudaFuncSetAttribute(track_batch_kernel<NMV, PR, FF>,                           \
+  cudaFuncSetAttribute(track_batch_kernel<NMV, PR, FF, LN>,                       \
                        cudaFuncAttributeMaxDynamicSharedMemorySize, smax)
-#define PHC_LAUNCH(NMV, PR, FF, K, P)                                              \
-  K<NMV, PR, FF><<<grid, block, smem, s>>>(P)
-#define PHC_OCC(NMV, PR, FF, K)                                                    \
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, K<NMV, PR, FF>, block, smem)
+#define PHC_LAUNCH(NMV, PR, FF, LN, K, P)                                          \
+  K<NMV, PR, FF, LN><<<grid, block, smem, s>>>(P)
+#define PHC_OCC(NMV, PR, FF, LN, K)                                                \
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, K<NMV, PR, FF, LN>, block, smem)
 
 #define PHC_DEFINE_NM(NMV)                                                        \
   namespace phc {                                                                 \
@@ -1275,7 +1309,7 @@ __global__ void __launch_bounds__(kMaxBlockThreads<NM>)
     if (dev >= 0 && dev < 64 && !done[dev]) {                                     \
       int smax = 0;                                                               \
       cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev); \
-      for (int mode = 0; mode < 6; ++mode) {                                      \
+      for (int mode = 0; mode < 12; ++mode) {                                     \
         PHC_FOR_MODES(PHC_SET_ATTR, NMV, smax)                                    \
       }                                                                           \
       done[dev] = 1;                                                              \

@@ -20,10 +20,10 @@ namespace phc {
 namespace {
 
 struct TuneKey {
-  int device, precision, schedule, nm;
+  int device, precision, schedule, nm, lean;
   bool operator<(const TuneKey& o) const {
-    return std::tie(device, precision, schedule, nm) <
-           std::tie(o.device, o.precision, o.schedule, o.nm);
+    return std::tie(device, precision, schedule, nm, lean) <
+           std::tie(o.device, o.precision, o.schedule, o.nm, o.lean);
   }
 };
 struct TuneVal {
@@ -34,9 +34,10 @@ std::map<TuneKey, TuneVal> g_tuned;
 
 }  // namespace
 
-bool tuned_launch(int device, int precision, int schedule, int nm, int* warps, int* chunk) {
+bool tuned_launch(int device, int precision, int schedule, int nm, int lean, int* warps,
+                  int* chunk) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  auto it = g_tuned.find(TuneKey{device, precision, schedule, nm});
+  auto it = g_tuned.find(TuneKey{device, precision, schedule, nm, lean});
   if (it == g_tuned.end()) return false;
   *warps = it->second.warps;
   *chunk = it->second.chunk;
@@ -116,7 +117,9 @@ extern "C" int32_t phc_autotune(const phc_system* sys, const phc_solve_options* 
         gc.chunk = chunks[ci];
         gc.precision = prec;
         LaunchCfg cfg;
-        if (resolve_launch(hp, gc, g.device, &cfg) != PHC_OK || cfg.warps != w) continue;
+        // the form a plan of the whole system uses (phc_plan_create)
+        if (resolve_launch(hp, gc, g.device, hp.nstart, &cfg) != PHC_OK || cfg.warps != w)
+          continue;
         phc_plan* plan = nullptr;
         st = phc_plan_create(sys, &hv, &so, &gc, &plan);
         if (st != PHC_OK) {
@@ -159,7 +162,8 @@ extern "C" int32_t phc_autotune(const phc_system* sys, const phc_solve_options* 
   gpu->precision = prec;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[TuneKey{g.device, prec, gpu->schedule == PHC_SCHED_PERSISTENT ? 1 : 0, nm}] =
+    g_tuned[TuneKey{g.device, prec, gpu->schedule == PHC_SCHED_PERSISTENT ? 1 : 0, nm,
+                    use_lean(hp.nstart, g.device) ? 1 : 0}] =
         TuneVal{gpu->warps_per_block, gpu->chunk};
   }
   if (report) *report = rep;
