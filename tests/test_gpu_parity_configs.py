@@ -15,10 +15,14 @@ modes:
     full-size property tests).
 
 Criteria are those of the reference's solve() contract: identical status,
-winding number, end game status, at-infinity / singular / real
-classification and solution indices per path; identical counts; finite
-regular endpoints within 1e-10 relative (max norm), singular solution sets
-within 1e-6 (the reference's singular_dedup_tol)."""
+winding number, at-infinity / singular / real classification and solution
+indices per path; identical counts; finite regular endpoints within 1e-10
+relative (max norm), singular solution sets within 1e-6 (the reference's
+singular_dedup_tol). The end game status is identical too, except on
+paths at infinity whose end game errors on both sides are at most 1e-7: the
+flag compares them with 1e-11, and rounding decides it there (a few
+cyclic-6 paths, with the round-one kernel as with this one). No path may
+take pathologically more steps than the restatement's."""
 import os
 
 import numpy as np
@@ -26,7 +30,8 @@ import pytest
 
 import polyhomocont_b200 as P
 from polyhomocont_b200 import workloads as W
-from tests.helpers import TOL_REGULAR, assert_parity
+from tests.helpers import (TOL_REGULAR, assert_parity, assert_steps_comparable,
+                           endgame_status_agrees)
 
 pytestmark = pytest.mark.gpu
 
@@ -35,8 +40,7 @@ NT = os.cpu_count() or 4
 STREAM_PER_SIZE = 10
 CFG5_WINDOWS = 8
 CFG5_WINDOW = 128
-PATH_KEYS = ("status", "winding_number", "endgame_status", "at_infinity", "singular",
-             "is_real")
+PATH_KEYS = ("status", "winding_number", "at_infinity", "singular", "is_real")
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -184,6 +188,9 @@ def test_large_system_windows(cfg5_ref, precision):
         for key in PATH_KEYS:
             bad = np.nonzero(pg[key] != pr[key])[0]
             assert bad.size == 0, (k0, key, (bad + k0)[:10])
+        ok = endgame_status_agrees(pr, pg)
+        assert ok.all(), (k0, "endgame_status", (np.nonzero(~ok)[0] + k0)[:10])
+        assert_steps_comparable(pr, pg)
         fin = (pr["status"] == 0) & (pr["at_infinity"] == 0) & (pr["singular"] == 0)
         assert fin.any()
         d = np.max(np.abs(xg[fin] - xr[fin]), axis=1) / np.maximum(
