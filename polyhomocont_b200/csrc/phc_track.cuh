@@ -327,14 +327,6 @@ enum Pc : int {
 };
 
 constexpr double kPi = 3.14159265358979323846;
-// Mixed precision: an FP32 step attempt that fails is redone in FP64 (and
-// the path stays in FP64 for a few steps) only if its last Newton update
-// was at most kFp32Redo ||z||. A larger update means the corrector was
-// still far from converging: the step was too large, and the FP64 attempt
-// rejects it too. On the n = 16, 65,536-path system every FP32 failure
-// whose FP64 redo succeeded had a last update below 1e-6 ||z|| (99.6%
-// below 1e-8); 99.3% of all FP64 redos failed.
-constexpr double kFp32Redo = 1.0e-6;
 constexpr double kEps = DBL_EPSILON;
 constexpr double kTiny = DBL_MIN;
 constexpr double kHuge = DBL_MAX;
@@ -541,9 +533,6 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
 
         case PC_SEG_AFTER_UNIT: {
           int outcome = 0;  // 1 accept, 2 reject
-          // a failed FP32 attempt whose last Newton update is larger than
-          // FP32 rounding can explain is a genuine rejection
-          bool beyond_fp32 = false;
           if (stage < 4) {
             ++st.c_tan;
             if (!U.ok) {
@@ -596,7 +585,6 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
               // ||dz|| <= tol ||z|| and the contraction test on squared norms
               const double d2 = vnorm2(U.x, lane, N);
               const double z2 = vnorm2(zp, lane, N);
-              beyond_fp32 = d2 > (kFp32Redo * kFp32Redo) * z2;
               if (d2 <= (TO.corrector_tol * TO.corrector_tol) * z2) {
                 outcome = 1;
               } else if (it > 1 && d2 > (TO.contraction * TO.contraction) * dnorm_prev) {
@@ -627,10 +615,9 @@ __device__ __forceinline__ void track_one(const unsigned char* tbl, unsigned cha
             }
             pc = PC_SEG_ATTEMPT;
           } else {
-            if (kMixed && !att64 && !beyond_fp32) {
-              // the FP32 attempt failed within FP32 rounding: redo the same
-              // step in FP64 before counting a rejection, and stay in FP64
-              // for a few steps
+            if (kMixed && !att64) {
+              // the FP32 attempt failed: redo the same step in FP64 before
+              // counting a rejection, and stay in FP64 for a few steps
               att64 = true;
               st.sticky = O.fp64_sticky;
               stage = 0;
