@@ -207,7 +207,7 @@ bool use_lean(int64_t paths, int device) {
 
 int resolve_launch(const HostPlan& hp, const phc_gpu_options& g, int device, int64_t paths,
                    LaunchCfg* cfg) {
-  cfg->nm = pick_nm(eliminated_rows(hp.n));
+  cfg->nm = kernel_nm(hp.n);
   cfg->lean = use_lean(paths, device) ? 1 : 0;
   if (cfg->nm == 0) {
     set_last_error("more than 32 unknowns");

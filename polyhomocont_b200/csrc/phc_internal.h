@@ -220,15 +220,18 @@ PHC_HD inline WsLayout ws_layout(int n, int S, int pw_size, bool eval32) {
   return L;
 }
 
-// Supported register-row widths: the compile-time capacity NM of the rows
-// of the eliminated system, N = n + 1 rows, or n when the patch row is
-// eliminated first.
+// Supported register-row widths: the compile-time capacity NM of the N =
+// n + 1 rows of the eliminated system.
 constexpr int kNMs[] = {6, 8, 12, 16, 18, 24, 32};
 inline int pick_nm(int rows) {
   for (int v : kNMs)
     if (rows <= v) return v;
   return 0;
 }
+// The kernel family of n = 16 with the patch row eliminated first: 16 rows
+// of 16 columns (RowLayout), its own width id so that the reduction is
+// compiled into these kernels only and no kernel carries both forms.
+constexpr int kNmReduced16 = 17;
 // The patch row is eliminated first where that moves the system into a
 // layout with more lanes per row: 17 unknowns have 16 equation rows, which
 // fit the two-lane layout (rows of up to 16). (For 9 unknowns the same would
@@ -236,7 +239,8 @@ inline int pick_nm(int rows) {
 // path that the other form fails in 14,000 units into one that fails in the
 // end game after 3.2 million, so n = 8 keeps the patch as a row.)
 PHC_HD constexpr bool reduce_patch_row(int n) { return n == 16; }
-PHC_HD constexpr int eliminated_rows(int n) { return reduce_patch_row(n) ? n : n + 1; }
+// The kernel width for a system of n equations.
+inline int kernel_nm(int n) { return reduce_patch_row(n) ? kNmReduced16 : pick_nm(n + 1); }
 // The single-system kernels of rows up to 8 columns carry an FP32
 // evaluation for the mixed predictor; every other kernel evaluates in FP64.
 PHC_HD constexpr bool kernel_eval32(int nm, int precision) {

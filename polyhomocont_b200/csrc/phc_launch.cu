@@ -17,6 +17,7 @@ PHC_DECLARE_NM(6)
 PHC_DECLARE_NM(8)
 PHC_DECLARE_NM(12)
 PHC_DECLARE_NM(16)
+PHC_DECLARE_NM(17)
 PHC_DECLARE_NM(18)
 PHC_DECLARE_NM(24)
 PHC_DECLARE_NM(32)
@@ -30,6 +31,7 @@ cudaError_t launch_track(const LaunchCfg& cfg, const KParams& kp, int grid, cuda
     case 8: return launch_nm_8(mode, kp, grid, block, cfg.smem, s);
     case 12: return launch_nm_12(mode, kp, grid, block, cfg.smem, s);
     case 16: return launch_nm_16(mode, kp, grid, block, cfg.smem, s);
+    case 17: return launch_nm_17(mode, kp, grid, block, cfg.smem, s);
     case 18: return launch_nm_18(mode, kp, grid, block, cfg.smem, s);
     case 24: return launch_nm_24(mode, kp, grid, block, cfg.smem, s);
     case 32: return launch_nm_32(mode, kp, grid, block, cfg.smem, s);
@@ -45,6 +47,7 @@ int track_blocks_per_sm(const LaunchCfg& cfg) {
     case 8: return occupancy_nm_8(mode, block, cfg.smem);
     case 12: return occupancy_nm_12(mode, block, cfg.smem);
     case 16: return occupancy_nm_16(mode, block, cfg.smem);
+    case 17: return occupancy_nm_17(mode, block, cfg.smem);
     case 18: return occupancy_nm_18(mode, block, cfg.smem);
     case 24: return occupancy_nm_24(mode, block, cfg.smem);
     case 32: return occupancy_nm_32(mode, block, cfg.smem);
@@ -62,6 +65,7 @@ cudaError_t launch_track_batch(int nm, int prec, int fac, int lean, int warps, i
     case 8: return launch_batch_nm_8(mode, kb, grid, block, smem, s);
     case 12: return launch_batch_nm_12(mode, kb, grid, block, smem, s);
     case 16: return launch_batch_nm_16(mode, kb, grid, block, smem, s);
+    case 17: return launch_batch_nm_17(mode, kb, grid, block, smem, s);
     case 18: return launch_batch_nm_18(mode, kb, grid, block, smem, s);
     case 24: return launch_batch_nm_24(mode, kb, grid, block, smem, s);
     case 32: return launch_batch_nm_32(mode, kb, grid, block, smem, s);
@@ -77,6 +81,7 @@ int track_batch_blocks_per_sm(int nm, int prec, int fac, int lean, int warps, in
     case 8: return occupancy_batch_nm_8(mode, block, smem);
     case 12: return occupancy_batch_nm_12(mode, block, smem);
     case 16: return occupancy_batch_nm_16(mode, block, smem);
+    case 17: return occupancy_batch_nm_17(mode, block, smem);
     case 18: return occupancy_batch_nm_18(mode, block, smem);
     case 24: return occupancy_batch_nm_24(mode, block, smem);
     case 32: return occupancy_batch_nm_32(mode, block, smem);

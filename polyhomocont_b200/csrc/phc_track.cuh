@@ -83,9 +83,13 @@ __device__ __forceinline__ WarpState* warp_state(const PlanHeader& P, unsigned c
 
 template <int NM>
 struct RowLayout {
-  static constexpr int kLanes = NM <= 8 ? 4 : (NM <= 16 ? 2 : 1);  // lanes per row
+  // the kernels of width kNmReduced16 hold 16 rows of 16 columns, the
+  // reduced system of n = 16 with the patch row eliminated first
+  static constexpr bool kReduce = NM == kNmReduced16;
+  static constexpr int kCols = kReduce ? 16 : NM;
+  static constexpr int kLanes = kCols <= 8 ? 4 : (kCols <= 16 ? 2 : 1);  // lanes per row
   static constexpr bool kSplit = kLanes > 1;
-  static constexpr int kRegs = kLanes == 4 ? 2 : (kLanes == 2 ? NM / 2 : NM);  // per lane
+  static constexpr int kRegs = kLanes == 4 ? 2 : (kLanes == 2 ? kCols / 2 : kCols);  // per lane
   static constexpr int kRows = 32 / kLanes;  // rows per warp
 };
 
@@ -154,7 +158,7 @@ __device__ __forceinline__ void run_unit(const unsigned char* tbl, const WarpCon
   constexpr int S = L::kLanes;
   const PlanHeader& P = *reinterpret_cast<const PlanHeader*>(tbl);
   const int n = C.n, N = C.N, c = C.red_c;
-  const bool reduce = P.reduce != 0;
+  constexpr bool reduce = L::kReduce;
   const int rows = reduce ? n : N;  // rows of the eliminated system
   // the row this lane works on (rows >= `rows` hold zeros), and whether it
   // reports the row (part 0)

@@ -74,7 +74,7 @@ extern "C" int32_t phc_autotune(const phc_system* sys, const phc_solve_options* 
   st = build_plan(sys, &hv, &hp);
   if (st != PHC_OK) return st;
   const int prec = (g.precision == PHC_PREC_MIXED) ? PHC_PREC_MIXED : PHC_PREC_FP64;
-  const int nm = pick_nm(eliminated_rows(hp.n));
+  const int nm = kernel_nm(hp.n);
   int64_t sample = sample_paths;
   if (sample <= 0) sample = (int64_t)device_sms(g.device) * 8 * 4;
   sample = std::min<int64_t>(sample, hp.nstart);
