@@ -201,8 +201,12 @@ int launch_batch(phc_server* S, Slot& s) {
     ws_cap = std::max(ws_cap, ws_layout(r.plan.n, r.plan.S, r.plan.pw_size, false).bytes);
   }
   const int slice = table_cap + ws_cap + align16((int)sizeof(KOpts));
-  // the lean kernel form for batches with many more paths than resident warps
-  const int lean = use_lean(total, S->cfg.device) ? 1 : 0;
+  // the lean kernel form for batches with many more paths than resident
+  // warps, of systems with rows of at least 16 columns: for smaller rows
+  // the form's register savings buy less than its extra work per unit
+  // costs (the serving stream of n <= 8: 1,577 systems/s lean against
+  // 2,075 not)
+  const int lean = (nm >= 16 && use_lean(total, S->cfg.device)) ? 1 : 0;
   const int smax = device_smem_optin(S->cfg.device);
   int warps = g.warps_per_block > 0
                   ? std::min(std::max(g.warps_per_block, 1), max_warps_per_block(nm, lean != 0))
