@@ -188,11 +188,17 @@ def endgame_status_agrees(ref_paths, got_paths):
 
 def assert_steps_comparable(ref_paths, got_paths):
     """No path takes pathologically more steps than the restatement's: at
-    most twice its steps plus 1000, and the total within 10 %. (The step
-    sequences coincide for most paths; rounding changes a few.)"""
+    most twice its steps plus 1000; on the paths at infinity whose end game
+    flag rounding decides (endgame_status_agrees), where one side may
+    converge early and the other continue down to the smallest radius, at
+    most 8 times plus 5000. The total stays within 10 %."""
     rs = ref_paths["naccepted"].astype(np.int64) + ref_paths["nrejected"]
     gs = got_paths["naccepted"].astype(np.int64) + got_paths["nrejected"]
-    bad = np.nonzero(gs > 2 * rs + 1000)[0]
+    band = ((ref_paths["at_infinity"] != 0) & (got_paths["at_infinity"] != 0) &
+            (ref_paths["endgame_error"] <= ENDGAME_FLAG_BAND) &
+            (got_paths["endgame_error"] <= ENDGAME_FLAG_BAND))
+    limit = np.where(band, 8 * rs + 5000, 2 * rs + 1000)
+    bad = np.nonzero(gs > limit)[0]
     assert bad.size == 0, ("steps", bad[:10], gs[bad[:10]], rs[bad[:10]])
     assert gs.sum() <= 1.1 * rs.sum() + 1000, (gs.sum(), rs.sum())
 
