@@ -259,19 +259,21 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
+# mixed-precision launch of the tracker on the first 6,144 paths of the
+# n = 16 system, from
+#   ncu --set full --clock-control none -k regex:track_kernel -s 6 -c 2
+#   python bench.py --max-paths 6144 --no-tune --steps 1 --warmup 3 --no-cpu
+#       --no-e2e --no-n10 --serving-systems 0
+# The kernel is compute- and latency-bound: its DRAM traffic is the table,
+# the kernel's code and the path records, most of which stay in L2.
+NCU_DRAM_BYTES = {"bytes": 204288, "paths": 6144}
+SCHED_NAMES = {0: "grid", 1: "persistent"}
+
+
 # ---------------------------------------------------------------------------
 # serving: stream of random sparse systems (n ~ U{2..8}, d_i ~ U{2,3})
 # ---------------------------------------------------------------------------
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
-# mixed-precision launch of the tracker on the first 4,736 paths of this
-# system, from
-#   ncu --set full --clock-control none -k regex:track_kernel -s 3 -c 1
-#   python bench.py --configs --config-filter large --max-paths 4736 --no-tune
-#       --steps 1 --warmup 3
-# The kernel is compute- and latency-bound: its DRAM traffic is the table,
-# the kernel's code and the path records, most of which stay in L2.
-NCU_DRAM_BYTES = {"bytes": 521728, "paths": 4736}
-SCHED_NAMES = {0: "grid", 1: "persistent"}
 
 
 def serving(P, W, nsys, device, load=0.7, nslots=16, max_batch_systems=64,
