@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--no-tune", action="store_true",
                     help="default launch configuration instead of the autotuner's "
                          "(for profiling: the timed launches then follow the warm-up directly)")
+    ap.add_argument("--warps-per-block", type=int, default=0,
+                    help="with --no-tune: warps per block of both arms (0: the default)")
     return ap.parse_args()
 
 
@@ -555,8 +557,9 @@ def main():
     # a sample of the system's paths, before and outside the timed region);
     # the two arms then differ only in precision and in what the tuner chose
     if args.no_tune:
-        g_mixed = P.default_gpu_options(P.PHC_PREC_MIXED, device=local)
-        g_fp64 = P.default_gpu_options(P.PHC_PREC_FP64, device=local)
+        wpb = {"warps_per_block": args.warps_per_block} if args.warps_per_block > 0 else {}
+        g_mixed = P.default_gpu_options(P.PHC_PREC_MIXED, device=local, **wpb)
+        g_fp64 = P.default_gpu_options(P.PHC_PREC_FP64, device=local, **wpb)
         tune_m = {"sample_paths": 0, "candidates": []}
     else:
         g_mixed, tune_m = P.autotune(sysP, gpu=P.default_gpu_options(P.PHC_PREC_MIXED,

@@ -247,15 +247,16 @@ PHC_HD constexpr bool kernel_eval32(int nm, int precision) {
   return precision == PHC_PREC_MIXED && nm <= 8;
 }
 // Most warps per block of the tracking kernels. The lean form (the path
-// state out of registers across a unit, see track_one) of rows of up to 18
-// columns is compiled for blocks of up to 12 warps, so that 12 warps share
-// one staged copy of the table; that bounds its registers at 65,536 / 384 =
-// 170 per thread, which it fits without spilling. The other kernels are
-// compiled for blocks of up to 8 warps (255 registers).
+// state out of registers across a unit, see track_one) is compiled for
+// larger blocks, so that more warps share one staged copy of the table:
+// rows of up to 17 columns for 16 warps (65,536 / 512 = 128 registers per
+// thread; the n = 16 family spills a few bytes at that bound, the narrower
+// ones need no more), rows of 18 for 12 warps (170 registers). The other
+// kernels are compiled for blocks of up to 8 warps (255 registers).
 PHC_HD constexpr int max_warps_per_block(int nm, bool lean) {
-  return lean && nm <= 18 ? 12 : 8;
+  return lean ? (nm <= 17 ? 16 : (nm <= 18 ? 12 : 8)) : 8;
 }
-constexpr int kMaxWarpsPerBlock = 12;  // over all kernels
+constexpr int kMaxWarpsPerBlock = 16;  // over all kernels
 // Resident warps per SM below which a launch is latency-bound: the form
 // that keeps the path state in registers is used for launches of at most
 // twice that many paths per SM, the lean form above.

@@ -2,7 +2,7 @@
 // the per-process table of tuned values that resolve_launch consults.
 //
 // Candidates are every schedule (persistent refill, one path per warp),
-// warps per block in {1, 2, 4, 6, 8, 12} that fit in shared memory, and refill
+// warps per block in {1, 2, 4, 6, 8, 12, 16} that fit in shared memory, and refill
 // chunks {1, 2, 4} for the persistent schedule. Each is timed with CUDA
 // events on the same sample of paths (one untimed launch, then the best of
 // two timed ones), and the fastest wins.
@@ -105,7 +105,7 @@ extern "C" int32_t phc_autotune(const phc_system* sys, const phc_solve_options* 
   rep.sample_paths = sample;
   rep.best = -1;
   const int scheds[2] = {PHC_SCHED_PERSISTENT, PHC_SCHED_GRID};
-  const int warps_c[6] = {1, 2, 4, 6, 8, 12};
+  const int warps_c[7] = {1, 2, 4, 6, 8, 12, 16};
   const int chunks[3] = {1, 2, 4};
   for (int sch : scheds) {
     for (int w : warps_c) {

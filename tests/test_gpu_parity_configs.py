@@ -21,8 +21,8 @@ relative (max norm), singular solution sets within 1e-6 (the reference's
 singular_dedup_tol). The end game status is identical too, except on
 paths at infinity whose end game errors on both sides are at most 1e-7: the
 flag compares them with 1e-11, and rounding decides it there (a few
-cyclic-6 paths, with the round-one kernel as with this one). No path may
-take pathologically more steps than the restatement's."""
+cyclic-6 paths, with every form of the kernel). No path may take
+pathologically more steps than the restatement's."""
 import os
 
 import numpy as np
