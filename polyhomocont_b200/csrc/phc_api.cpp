@@ -430,8 +430,8 @@ class PointSet {
   // rho = tol * max(1, ||x||) comes from the norm estimate; the decisions
   // it makes keep a relative margin of 1e-12, far above the estimate's
   // error, and the few comparisons inside the margin use the exact norm.
-  int find(const double* x) const {
-    const double est = norm_inf_estimate(x, n_);
+  // est: norm_inf_estimate(x, n) (the caller has it already).
+  int find(const double* x, double est) const {
     const bool approx = std::isfinite(est);
     const double rho = tol_ * std::max(1.0, approx ? est : norm_inf_c(x, n_));
     double rho_exact = approx ? -1.0 : rho;  // computed on first need
@@ -544,11 +544,30 @@ class PointSet {
   std::vector<int> special_;
 };
 
+// collect_real's test for one solution (src/solve.f90:402-426):
+// max_i |Im s_i| <= real_tol * max(1, ||s||), with the norm estimate
+// deciding away from the threshold.
+static bool is_real_solution(const double* s, int n, double est, double real_tol) {
+  double imax = 0.0;
+  for (int i = 0; i < n; ++i) imax = std::max(imax, std::fabs(s[2 * i + 1]));
+  const double thr = real_tol * std::max(1.0, est);
+  if (std::isfinite(est) && imax <= thr * (1.0 - kSqMargin)) return true;
+  if (std::isfinite(est) && imax >= thr * (1.0 + kSqMargin)) return false;
+  return imax <= real_tol * std::max(1.0, norm_inf_c(s, n));
+}
+
+// One pass in path order: each endpoint's norm estimate serves its dedup
+// query and, for a new regular solution, collect_real's test; new
+// solutions are copied out as they are found. collect_real runs over the
+// solutions in index order, which is the order they are found in, so the
+// real list is the same.
 void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out* paths,
                  const double* x, phc_solve_result* res) {
   phc_solve_counts& c = res->counts;
   PointSet sols(n, o.dedup_tol, x, npaths), ssols(n, o.singular_dedup_tol, x, 64);
   std::vector<int> mult;
+  const size_t row = (size_t)2 * n * sizeof(double);
+  int nreal = 0;
   for (int64_t k = 0; k < npaths; ++k) {
     phc_path_out& p = paths[k];
     const double* xk = x + (size_t)k * 2 * n;
@@ -559,59 +578,39 @@ void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out
     } else if (p.at_infinity) {
       c.ninfinite++;
     } else if (p.singular) {  // add_singular, src/solve.f90:353-377
-      int j = ssols.find(xk);
+      int j = ssols.find(xk, norm_inf_estimate(xk, n));
       if (j > 0) {
         mult[j - 1]++;
       } else {
         ssols.add(k);
         mult.push_back(1);
         j = ssols.size();
+        if (res->singular_solutions)
+          std::memcpy(res->singular_solutions + (size_t)(j - 1) * 2 * n, xk, row);
       }
       p.singular_index = j;
     } else {  // add_solution, src/solve.f90:330-351
-      int j = sols.find(xk);
+      const double est = norm_inf_estimate(xk, n);
+      int j = sols.find(xk, est);
       if (j > 0) {
         c.nduplicates++;
       } else {
         sols.add(k);
         j = sols.size();
+        if (res->solutions) std::memcpy(res->solutions + (size_t)(j - 1) * 2 * n, xk, row);
+        if (is_real_solution(xk, n, est, o.real_tol)) {
+          if (res->real_solutions)
+            for (int i = 0; i < n; ++i) res->real_solutions[(size_t)nreal * n + i] = xk[2 * i];
+          ++nreal;
+        }
       }
       p.solution_index = j;
     }
   }
-  const int nsol = sols.size(), nsing = ssols.size();
-  c.nsolutions = nsol;
-  c.nsingular = nsing;
-  const size_t row = (size_t)2 * n * sizeof(double);
-  if (res->solutions)
-    for (int j = 0; j < nsol; ++j) std::memcpy(res->solutions + (size_t)j * 2 * n, sols.point(j), row);
-  if (res->singular_solutions)
-    for (int j = 0; j < nsing; ++j)
-      std::memcpy(res->singular_solutions + (size_t)j * 2 * n, ssols.point(j), row);
+  c.nsolutions = sols.size();
+  c.nsingular = ssols.size();
   if (res->multiplicities)
-    for (int j = 0; j < nsing; ++j) res->multiplicities[j] = mult[j];
-  // collect_real, src/solve.f90:402-426
-  int nreal = 0;
-  for (int j = 0; j < nsol; ++j) {
-    const double* sj = sols.point(j);
-    double imax = 0.0;
-    for (int i = 0; i < n; ++i) imax = std::max(imax, std::fabs(sj[2 * i + 1]));
-    // imax <= real_tol * max(1, ||s||), the norm estimated away from the threshold
-    const double est = norm_inf_estimate(sj, n);
-    bool real;
-    const double thr = o.real_tol * std::max(1.0, est);
-    if (std::isfinite(est) && imax <= thr * (1.0 - kSqMargin))
-      real = true;
-    else if (std::isfinite(est) && imax >= thr * (1.0 + kSqMargin))
-      real = false;
-    else
-      real = imax <= o.real_tol * std::max(1.0, norm_inf_c(sj, n));
-    if (real) {
-      if (res->real_solutions)
-        for (int i = 0; i < n; ++i) res->real_solutions[(size_t)nreal * n + i] = sj[2 * i];
-      ++nreal;
-    }
-  }
+    for (int j = 0; j < c.nsingular; ++j) res->multiplicities[j] = mult[j];
   c.nreal = nreal;
 }
 
