@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <complex>
@@ -16,7 +17,9 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <chrono>
 #include <mutex>
+#include <thread>
 #include <new>
 #include <string>
 #include <vector>
@@ -262,11 +265,35 @@ struct DevBuf {
     return PHC_OK;
   }
 };
+// Page-locked host memory mapped into the device's address space: the
+// kernel writes results into it directly (phc_solve_sparse).
+struct MappedBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t need) {
+    if (need <= cap) return PHC_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(need, (size_t)4096);
+    want += want / 2;
+    cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocMapped);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc(mapped results)");
+    cap = want;
+    return PHC_OK;
+  }
+  template <class T>
+  int device_ptr(T** d) const {
+    cudaError_t e = cudaHostGetDevicePointer(reinterpret_cast<void**>(d), p, 0);
+    return e == cudaSuccess ? PHC_OK : cuda_fail(e, "cudaHostGetDevicePointer");
+  }
+};
 struct DeviceWS {
   std::mutex mu;
   bool ready = false;
   cudaStream_t stream = nullptr;
   DevBuf plan, out, z, x, counter;
+  MappedBuf hout, hz, hx, hdone;
   unsigned char* stage = nullptr;  // pinned staging of the table upload
   size_t stage_cap = 0;
 };
@@ -560,17 +587,21 @@ static bool is_real_solution(const double* s, int n, double est, double real_tol
 // query and, for a new regular solution, collect_real's test; new
 // solutions are copied out as they are found. collect_real runs over the
 // solutions in index order, which is the order they are found in, so the
-// real list is the same.
-void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out* paths,
-                 const double* x, phc_solve_result* res) {
-  phc_solve_counts& c = res->counts;
-  PointSet sols(n, o.dedup_tol, x, npaths), ssols(n, o.singular_dedup_tol, x, 64);
-  std::vector<int> mult;
-  const size_t row = (size_t)2 * n * sizeof(double);
-  int nreal = 0;
-  for (int64_t k = 0; k < npaths; ++k) {
-    phc_path_out& p = paths[k];
-    const double* xk = x + (size_t)k * 2 * n;
+// real list is the same. Paths are added one at a time (add), so the pass
+// can run while later paths are still being tracked; x is the caller's
+// endpoint array, whose row k must hold path k's endpoint when it is added.
+class Bookkeeper {
+ public:
+  Bookkeeper(int n, int64_t npaths, const phc_solve_options& o, const double* x,
+             phc_solve_result* res)
+      : n_(n), o_(o), x_(x), res_(res), sols_(n, o.dedup_tol, x, npaths),
+        ssols_(n, o.singular_dedup_tol, x, 64) {}
+
+  void add(int64_t k, phc_path_out& p) {
+    phc_solve_counts& c = res_->counts;
+    const int n = n_;
+    const double* xk = x_ + (size_t)k * 2 * n;
+    const size_t row = (size_t)2 * n * sizeof(double);
     p.solution_index = 0;
     p.singular_index = 0;
     if (p.status != PHC_PATH_SUCCESS) {
@@ -578,40 +609,166 @@ void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out
     } else if (p.at_infinity) {
       c.ninfinite++;
     } else if (p.singular) {  // add_singular, src/solve.f90:353-377
-      int j = ssols.find(xk, norm_inf_estimate(xk, n));
+      int j = ssols_.find(xk, norm_inf_estimate(xk, n));
       if (j > 0) {
-        mult[j - 1]++;
+        mult_[j - 1]++;
       } else {
-        ssols.add(k);
-        mult.push_back(1);
-        j = ssols.size();
-        if (res->singular_solutions)
-          std::memcpy(res->singular_solutions + (size_t)(j - 1) * 2 * n, xk, row);
+        ssols_.add(k);
+        mult_.push_back(1);
+        j = ssols_.size();
+        if (res_->singular_solutions)
+          std::memcpy(res_->singular_solutions + (size_t)(j - 1) * 2 * n, xk, row);
       }
       p.singular_index = j;
     } else {  // add_solution, src/solve.f90:330-351
       const double est = norm_inf_estimate(xk, n);
-      int j = sols.find(xk, est);
+      int j = sols_.find(xk, est);
       if (j > 0) {
         c.nduplicates++;
       } else {
-        sols.add(k);
-        j = sols.size();
-        if (res->solutions) std::memcpy(res->solutions + (size_t)(j - 1) * 2 * n, xk, row);
-        if (is_real_solution(xk, n, est, o.real_tol)) {
-          if (res->real_solutions)
-            for (int i = 0; i < n; ++i) res->real_solutions[(size_t)nreal * n + i] = xk[2 * i];
-          ++nreal;
+        sols_.add(k);
+        j = sols_.size();
+        if (res_->solutions) std::memcpy(res_->solutions + (size_t)(j - 1) * 2 * n, xk, row);
+        if (is_real_solution(xk, n, est, o_.real_tol)) {
+          if (res_->real_solutions)
+            for (int i = 0; i < n; ++i) res_->real_solutions[(size_t)nreal_ * n + i] = xk[2 * i];
+          ++nreal_;
         }
       }
       p.solution_index = j;
     }
   }
-  c.nsolutions = sols.size();
-  c.nsingular = ssols.size();
-  if (res->multiplicities)
-    for (int j = 0; j < c.nsingular; ++j) res->multiplicities[j] = mult[j];
-  c.nreal = nreal;
+
+  void finish() {
+    phc_solve_counts& c = res_->counts;
+    c.nsolutions = sols_.size();
+    c.nsingular = ssols_.size();
+    if (res_->multiplicities)
+      for (int j = 0; j < c.nsingular; ++j) res_->multiplicities[j] = mult_[j];
+    c.nreal = nreal_;
+  }
+
+ private:
+  int n_;
+  phc_solve_options o_;
+  const double* x_;
+  phc_solve_result* res_;
+  PointSet sols_, ssols_;
+  std::vector<int> mult_;
+  int nreal_ = 0;
+};
+
+void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out* paths,
+                 const double* x, phc_solve_result* res) {
+  Bookkeeper b(n, npaths, o, x, res);
+  for (int64_t k = 0; k < npaths; ++k) b.add(k, paths[k]);
+  b.finish();
+}
+
+// solve()'s tracking and bookkeeping overlapped (src/solve.f90:190-213):
+// the kernel writes every path's record, z and x into mapped host memory
+// and then flags the path (KParams::done); this thread takes the paths in
+// order as their flags appear, copies them into the caller's arrays and
+// runs the bookkeeping on each, so that when the last path finishes only
+// its own bookkeeping is left. The results are identical to tracking all
+// paths first and running the bookkeeping afterwards.
+int solve_streamed(const HostPlan& hp, const phc_solve_options& so, const phc_gpu_options& g,
+                   int64_t count, phc_solve_result* res) {
+  int st = check_device(g.device);
+  if (st != PHC_OK) return st;
+  Bookkeeper book(hp.n, count, so, res->x, res);
+  if (count <= 0) {
+    book.finish();
+    return PHC_OK;
+  }
+  DeviceWS& W = g_ws[g.device];
+  std::lock_guard<std::mutex> lock(W.mu);
+  PHC_CUDA(cudaSetDevice(g.device));
+  if (!W.ready) {
+    PHC_CUDA(cudaStreamCreateWithFlags(&W.stream, cudaStreamNonBlocking));
+    W.ready = true;
+  }
+  LaunchCfg cfg;
+  st = resolve_launch(hp, g, g.device, count, &cfg);
+  if (st != PHC_OK) return st;
+  const size_t zrow = (size_t)hp.N * 2, xrow = (size_t)hp.n * 2;
+  if ((st = W.plan.ensure(hp.bytes.size() + 16)) != PHC_OK) return st;
+  if ((st = W.counter.ensure(16)) != PHC_OK) return st;
+  if ((st = W.hout.ensure((size_t)count * sizeof(phc_path_out))) != PHC_OK) return st;
+  if ((st = W.hz.ensure((size_t)count * zrow * sizeof(double))) != PHC_OK) return st;
+  if ((st = W.hx.ensure((size_t)count * xrow * sizeof(double))) != PHC_OK) return st;
+  if ((st = W.hdone.ensure((size_t)count * sizeof(unsigned int))) != PHC_OK) return st;
+  if (hp.bytes.size() > W.stage_cap) {
+    if (W.stage) cudaFreeHost(W.stage);
+    W.stage = nullptr;
+    W.stage_cap = 0;
+    PHC_CUDA(cudaMallocHost((void**)&W.stage, hp.bytes.size() * 2));
+    W.stage_cap = hp.bytes.size() * 2;
+  }
+  // the previous launch on these buffers has finished (this function
+  // returns only after its kernel), so the flags can be cleared here
+  volatile unsigned int* done = static_cast<volatile unsigned int*>(W.hdone.p);
+  std::memset(W.hdone.p, 0, (size_t)count * sizeof(unsigned int));
+  std::memcpy(W.stage, hp.bytes.data(), hp.bytes.size());
+  PHC_CUDA(cudaMemcpyAsync(W.plan.p, W.stage, hp.bytes.size(), cudaMemcpyHostToDevice, W.stream));
+  KParams kp;
+  std::memset(&kp, 0, sizeof(kp));
+  kp.plan = static_cast<const unsigned char*>(W.plan.p);
+  kp.plan_bytes = cfg.plan_bytes;
+  kp.ws_bytes = cfg.ws_bytes;
+  kp.warps = cfg.warps;
+  kp.persistent = cfg.persistent;
+  kp.chunk = cfg.chunk;
+  kp.k0 = 1;
+  kp.count = count;
+  kp.counter = static_cast<unsigned long long*>(W.counter.p);
+  if ((st = W.hout.device_ptr(&kp.out)) != PHC_OK) return st;
+  if ((st = W.hz.device_ptr(&kp.z)) != PHC_OK) return st;
+  if ((st = W.hx.device_ptr(&kp.x)) != PHC_OK) return st;
+  if ((st = W.hdone.device_ptr(&kp.done)) != PHC_OK) return st;
+  kp.opts = make_kopts(so, g);
+  int grid;
+  if (cfg.persistent) {
+    PHC_CUDA(cudaMemsetAsync(W.counter.p, 0, sizeof(unsigned long long), W.stream));
+    const int64_t need = (count + (int64_t)cfg.warps * cfg.chunk - 1) / ((int64_t)cfg.warps * cfg.chunk);
+    grid = (int)std::min<int64_t>(cfg.grid, need);
+  } else {
+    grid = (int)((count + cfg.warps - 1) / cfg.warps);
+  }
+  cudaError_t e = launch_track(cfg, kp, grid, W.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "track kernel launch");
+  const phc_path_out* hout = static_cast<const phc_path_out*>(W.hout.p);
+  const double* hz = static_cast<const double*>(W.hz.p);
+  const double* hx = static_cast<const double*>(W.hx.p);
+  bool finished = false;  // the kernel has completed: every flag is set
+  for (int64_t k = 0; k < count; ++k) {
+    // wait for path k: spin briefly, then sleep; ask the stream now and
+    // then, so that a failed launch ends the wait with its error
+    for (int spin = 0; !finished && done[k] == 0u; ++spin) {
+      if (spin < 256) continue;
+      e = cudaStreamQuery(W.stream);
+      if (e == cudaSuccess) {
+        finished = true;
+      } else if (e != cudaErrorNotReady) {
+        return cuda_fail(e, "track kernel");
+      } else {
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+      }
+    }
+    if (done[k] == 0u) {
+      set_last_error("track kernel finished without flagging a path");
+      return PHC_ERR_CUDA;
+    }
+    // the path's results were made visible before its flag
+    std::atomic_thread_fence(std::memory_order_acquire);
+    res->paths[k] = hout[k];
+    std::memcpy(res->z + (size_t)k * zrow, hz + (size_t)k * zrow, zrow * sizeof(double));
+    std::memcpy(res->x + (size_t)k * xrow, hx + (size_t)k * xrow, xrow * sizeof(double));
+    book.add(k, res->paths[k]);
+  }
+  PHC_CUDA(cudaStreamSynchronize(W.stream));
+  book.finish();
+  return PHC_OK;
 }
 
 }  // namespace phc
@@ -860,16 +1017,10 @@ int32_t phc_solve_sparse(const phc_system* sys, const phc_solve_options* opts,
     st = build_plan(sys, &hv, &hp);
     if (st != PHC_OK) return st;
   }
-  {
-    NvtxRange r("phc track: copies and kernel");
-    st = run_paths_sync(hp, so, g, 1, h.nstart, res->paths, res->z, res->x);
-    if (st != PHC_OK) return st;
-  }
   res->counts.n = sys->n;
   res->counts.npaths = (int32_t)h.nstart;
-  NvtxRange r("phc bookkeeping");
-  bookkeeping(sys->n, h.nstart, so, res->paths, res->x, res);
-  return PHC_OK;
+  NvtxRange r("phc track and bookkeeping");
+  return solve_streamed(hp, so, g, h.nstart, res);
 }
 
 // ---------------------------------------------------------------------------

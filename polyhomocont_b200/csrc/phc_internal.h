@@ -115,6 +115,10 @@ struct KParams {
   phc_path_out* out;          // [count]
   double* z;                  // [count][N][2]
   double* x;                  // [count][n][2] or null
+  // [count] or null: set to 1 (system scope) once path q's record, z and x
+  // are visible to the host; outputs in mapped host memory are then read
+  // while the launch runs
+  unsigned int* done;
   KOpts opts;
 };
 

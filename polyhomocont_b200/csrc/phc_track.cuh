@@ -1203,6 +1203,13 @@ __global__ void __launch_bounds__(kMaxBlockThreads<NM, LEAN>) track_kernel(const
     const int n = P.n, N = P.N;
     track_one<NM, PREC, E32, F, LEAN>(smem, wbase, *stp, kp.opts, kp.k0 + q, lane, kp.out + q,
                                       kp.z + 2 * q * N, kp.x ? kp.x + 2 * q * n : nullptr);
+    if (kp.done != nullptr) {
+      // every lane's result stores are made visible system-wide before the
+      // path is flagged
+      __threadfence_system();
+      __syncwarp();
+      if (lane == 0) atomicExch_system(&kp.done[q], 1u);
+    }
   }
 }
 

@@ -162,3 +162,30 @@ def test_wide_rows_parity_sample(orc, n):
             d = np.max(np.abs(xg[fin] - xr[fin]), axis=1) / np.maximum(
                 1.0, np.max(np.abs(xr[fin]), axis=1))
             assert d.max() <= TOL_REGULAR, (d.max(), prec)
+
+
+@pytest.mark.parametrize("precision", [P.PHC_PREC_FP64, P.PHC_PREC_MIXED])
+@pytest.mark.parametrize("name", ["cyclic5", "cfg3", "cfg2", "multiplicity4"])
+def test_streamed_solve_equals_tracking_then_bookkeeping(name, precision):
+    """phc_solve_sparse overlaps the bookkeeping with the tracking (the
+    kernel writes each path into mapped host memory and flags it); its
+    result must be byte-identical to tracking every path first
+    (phc_solve_paths) and running the bookkeeping afterwards
+    (phc_finish_solve), in both precisions and twice in a row (the second
+    call reuses the mapped buffers)."""
+    n, eqs = W.cfg2() if name == "cfg2" else CASES[name]
+    s = W.build(P.SparseSystem, n, eqs)
+    g = P.default_gpu_options(precision=precision)
+    pg, zg, xg, st = P.solve_paths(s, gpu=g)
+    assert st == 0
+    ref = P.result_from_arrays(n, pg, xg)
+    for _ in range(2):
+        got, st = P.solve(s, gpu=g)
+        assert st == 0
+        assert got.paths.tobytes() == ref.paths.tobytes()
+        assert np.array_equal(got.z.view(np.float64), np.asarray(zg).reshape(got.z.shape).view(np.float64))
+        assert np.array_equal(got.x.view(np.float64), np.asarray(xg).reshape(got.x.shape).view(np.float64))
+        for key in ("nsolutions", "nreal", "nsingular", "ninfinite", "nfailed", "nduplicates"):
+            assert getattr(got, key) == getattr(ref, key), key
+        for key in ("solutions", "real_solutions", "singular_solutions", "multiplicities"):
+            assert np.array_equal(getattr(got, key), getattr(ref, key)), key
