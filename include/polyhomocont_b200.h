@@ -11,7 +11,9 @@
  *   - runs start_solution + endpoint + classify for every path on the GPU
  *     (src/solve.f90:190-198, :217-328), one warp per path;
  *   - runs the order-dependent bookkeeping (add_solution, add_singular,
- *     find, collect_real; src/solve.f90:330-426) on the host in path order.
+ *     find, collect_real; src/solve.f90:330-426) on the host in path order,
+ *     path by path as the GPU finishes them (the kernel writes its results
+ *     into page-locked host memory that the library keeps per device).
  *
  * Conventions (all entry points):
  *   - plain C types; complex values are interleaved (re, im) doubles, like
@@ -261,7 +263,9 @@ void phc_default_gpu_options(phc_gpu_options* g);
 int64_t phc_bezout(const phc_system* sys);
 /* Whole solve: host set-up, GPU path numerics, host bookkeeping. Arrays in
  * *res are caller-allocated with capacity phc_bezout(sys) rows. opts or
- * gpu may be NULL (defaults). Returns the solve status. */
+ * gpu may be NULL (defaults). Returns the solve status. The bookkeeping of
+ * each path runs on the calling thread while later paths are tracked;
+ * calls on one device are serialized. */
 int32_t phc_solve_sparse(const phc_system* sys, const phc_solve_options* opts,
                          const phc_gpu_options* gpu, phc_solve_result* res);
 
