@@ -82,6 +82,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true",
                     help="default launch configuration instead of the autotuner's "
                          "(for profiling: the timed launches then follow the warm-up directly)")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="only the serving leg (--serving-systems systems, one GPU): "
+                         "one JSON line (for profiling the batch kernels)")
     ap.add_argument("--warps-per-block", type=int, default=0,
                     help="with --no-tune: warps per block of both arms (0: the default)")
     return ap.parse_args()
@@ -326,6 +329,22 @@ def serving(P, W, nsys, device, load=0.7, nslots=16, max_batch_systems=64,
             "slots": cfg["nslots"]}
 
 
+def run_serving_only(args):
+    """The serving leg alone on GPU 0: one JSON line."""
+    import torch
+    import polyhomocont_b200 as P
+    from polyhomocont_b200 import _abi
+    from polyhomocont_b200 import workloads as W
+    from polyhomocont_b200 import build as B
+
+    if not os.path.exists(_abi.LIB_PATH):
+        B.build()
+    torch.cuda.set_device(0)
+    serve = serving(P, W, max(args.serving_systems, 1), 0)
+    print(json.dumps({"impl": "ours", "metric": "serving stream (systems/s, latency)",
+                      "serving": serve}), flush=True)
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -499,6 +518,9 @@ def main():
         return
     if args.configs:
         run_configs(args)
+        return
+    if args.serving_only:
+        run_serving_only(args)
         return
     rank, world, local = dist_env()
     import torch
