@@ -672,8 +672,8 @@ void bookkeeping(int n, int64_t npaths, const phc_solve_options& o, phc_path_out
 // runs the bookkeeping on each, so that when the last path finishes only
 // its own bookkeeping is left. The results are identical to tracking all
 // paths first and running the bookkeeping afterwards.
-int solve_streamed(const HostPlan& hp, const phc_solve_options& so, const phc_gpu_options& g,
-                   int64_t count, phc_solve_result* res) {
+static int solve_streamed(const HostPlan& hp, const phc_solve_options& so, const phc_gpu_options& g,
+                          int64_t count, phc_solve_result* res) {
   int st = check_device(g.device);
   if (st != PHC_OK) return st;
   Bookkeeper book(hp.n, count, so, res->x, res);
