@@ -673,8 +673,9 @@ def main():
             def e2e_step():
                 res, _ = P.solve(sysP, gpu=g_mixed, buffers=bufs)
                 return res
-            how = ("phc_solve_sparse: host table in, page-locked host results out, host "
-                   "bookkeeping included")
+            how = ("phc_solve_sparse: host table in; each path's results written by the "
+                   "kernel to mapped host memory, copied into page-locked caller buffers and "
+                   "booked (host bookkeeping in path order) while later paths are tracked")
         else:
             def runner(kk, cc):
                 p_, z_, x_, st_ = P.solve_paths(sysP, gpu=g_mixed, k0=kk, count=cc)
