@@ -12,8 +12,9 @@ per-path work of one solve(). Metric: paths/s (higher is better).
           table) resident in device memory, timed with CUDA events on the
           launching stream, L2 flushed (256 MiB written) between timed steps
   e2e     the same metric through the public C ABI: phc_solve_sparse on one
-          GPU (host table in, host results out through page-locked buffers,
-          host bookkeeping included), wall clock per call; on N GPUs each
+          GPU (host table in; the kernel writes each path's results to mapped
+          host memory and the host copies and books it in path order while
+          later paths are tracked), wall clock per call; on N GPUs each
           rank calls phc_solve_paths on its path range with host buffers,
           the records are gathered to rank 0 and phc_finish_solve runs the
           bookkeeping there
